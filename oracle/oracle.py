@@ -1,0 +1,201 @@
+"""CPU oracle for the R^k / Y^k path — TEST INFRASTRUCTURE ONLY.
+
+Only the test-suite, ``__graft_entry__.smoke()`` (as the checker) and the
+benchmark's CPU-baseline leg import this module.  The engine never does.
+
+Each function restates the reference algorithm (atomx; paths are relative to
+its project root) in plain numpy or calls the C restatement in
+``rk_oracle.c``:
+
+* ``yk_partial_matrices``   <- src/atomx/numerics/yk.py:65-84
+* ``yk_rows`` / ``yk_row``  <- src/atomx/numerics/yk.py:88-154 (C, bit-faithful)
+* ``eval_orbital_on_grid``  <- src/atomx/numerics/bspline/evaluate.py:71-97
+* ``pair_density``          <- src/atomx/numerics/bspline/slater_yk.py:193-194
+* ``slater_rk_poisson``     <- src/atomx/numerics/bspline/slater.py:118-130
+* ``slater_rk_direct``      <- src/atomx/numerics/bspline/slater.py:51-115
+* ``dot_entries``           <- slater.py:130, one dot per ordered table entry
+
+Parity of the oracle itself is pinned against vectors generated by running
+the reference (tests/golden/make_golden.py) and against closed forms.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from functools import lru_cache
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "librk_oracle.so")
+
+_dptr = ctypes.POINTER(ctypes.c_double)
+_iptr = ctypes.POINTER(ctypes.c_int)
+_lptr = ctypes.POINTER(ctypes.c_long)
+
+
+def build() -> str:
+    """Compile the C oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+@lru_cache(maxsize=1)
+def _lib():
+    if not os.path.exists(_LIB_PATH) or (
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "rk_oracle.c"))):
+        build()
+    lib = ctypes.CDLL(_LIB_PATH)
+    lib.oracle_yk_rows.argtypes = [_dptr, _iptr, ctypes.c_long, _dptr, _dptr, ctypes.c_int,
+                                   ctypes.c_int, _dptr, _dptr, _dptr, ctypes.c_int]
+    lib.oracle_yk_rows.restype = None
+    lib.oracle_dot_table.argtypes = [_dptr, _dptr, ctypes.c_long, _lptr, _lptr, ctypes.c_long,
+                                     _dptr, ctypes.c_int]
+    lib.oracle_dot_table.restype = None
+    lib.oracle_int_pow.argtypes = [ctypes.c_double, ctypes.c_long]
+    lib.oracle_int_pow.restype = ctypes.c_double
+    lib.oracle_max_threads.restype = ctypes.c_int
+    return lib
+
+
+def max_threads() -> int:
+    return int(_lib().oracle_max_threads())
+
+
+def _p(a, ptr=_dptr):
+    return a.ctypes.data_as(ptr)
+
+
+@lru_cache(maxsize=32)
+def yk_partial_matrices(ng: int):
+    """Interpolatory partial-cell matrices (mo, mi = 1 - mo) for ``ng`` nodes.
+
+    mo[i, j] * w_j is the integral of the j-th Lagrange basis polynomial from
+    the cell's left edge to node i, evaluated through the orthogonal Legendre
+    expansion L_j(x)/w_j = sum_l (2l+1)/2 P_l(x_j) P_l(x) and the antiderivative
+    identity int_{-1}^x P_l = (P_{l+1} - P_{l-1})/(2l+1) (int P_0 = x + 1).
+    """
+    xi, _ = np.polynomial.legendre.leggauss(ng)
+    vand = np.polynomial.legendre.legvander(xi, ng)  # P_0..P_ng at the nodes
+    anti = np.empty((ng, ng))
+    anti[:, 0] = xi + 1.0
+    for ell in range(1, ng):
+        anti[:, ell] = (vand[:, ell + 1] - vand[:, ell - 1]) / (2 * ell + 1)
+    mo = (anti * ((2 * np.arange(ng) + 1) / 2.0)) @ vand[:, :ng].T
+    mo.setflags(write=False)
+    mi = 1.0 - mo
+    mi.setflags(write=False)
+    return mo, mi
+
+
+def yk_rows(rho: np.ndarray, ks, r: np.ndarray, w: np.ndarray, nv: int, ng: int,
+            threads: int = 0) -> np.ndarray:
+    """Y^k rows: ``rho`` is (nrows, nv*ng); ``ks`` a scalar or (nrows,) ints."""
+    rho = np.ascontiguousarray(np.atleast_2d(rho), dtype=np.float64)
+    nrows, n = rho.shape
+    assert n == nv * ng
+    ks = np.ascontiguousarray(np.broadcast_to(np.asarray(ks, dtype=np.int32), (nrows,)))
+    r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
+    w = np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+    mo, mi = yk_partial_matrices(ng)
+    mo = np.ascontiguousarray(mo)
+    mi = np.ascontiguousarray(mi)
+    out = np.empty_like(rho)
+    _lib().oracle_yk_rows(_p(rho), _p(ks, _iptr), nrows, _p(r), _p(w), nv, ng, _p(mo), _p(mi),
+                          _p(out), int(threads))
+    return out
+
+
+def yk_row(rho, r, w, nv, ng, k):
+    return yk_rows(np.asarray(rho).reshape(1, -1), k, r, w, nv, ng, threads=1)[0]
+
+
+def dot_entries(g: np.ndarray, y: np.ndarray, ia, ib, threads: int = 0) -> np.ndarray:
+    """out[e] = g[ia[e]] . y[ib[e]] with one plain dot per entry."""
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    ia = np.ascontiguousarray(ia, dtype=np.int64)
+    ib = np.ascontiguousarray(ib, dtype=np.int64)
+    out = np.empty(ia.shape[0])
+    _lib().oracle_dot_table(_p(g), _p(y), g.shape[1], _p(ia, _lptr), _p(ib, _lptr), ia.shape[0],
+                            _p(out), int(threads))
+    return out
+
+
+def eval_orbital_on_grid(coeffs: np.ndarray, bsp: np.ndarray, nv: int, ks: int, ns: int) -> np.ndarray:
+    """f(r_im) = sum_s c[i+s] B_s(r_im) with coefficients beyond ns taken as 0."""
+    coeffs = np.asarray(coeffs, dtype=np.float64)
+    idx = np.arange(nv)[:, None] + np.arange(ks)[None, :]
+    c = np.where(idx < ns, coeffs[np.minimum(idx, ns - 1)], 0.0)
+    return np.einsum("is,ims->im", c, bsp)
+
+
+def eval_P(coeffs, bsp_data):
+    return eval_orbital_on_grid(coeffs, bsp_data["bsp_p"], bsp_data["nv"], bsp_data["ksp"], bsp_data["nsp"])
+
+
+def eval_Q(coeffs, bsp_data):
+    return eval_orbital_on_grid(coeffs, bsp_data["bsp_q"], bsp_data["nv"], bsp_data["ksq"], bsp_data["nsq"])
+
+
+def pair_density(Pa, Qa, Pc, Qc):
+    """Dirac pair density rho_ac = P_a P_c + Q_a Q_c (node values)."""
+    return Pa * Pc + Qa * Qc
+
+
+def slater_rk_poisson(rho13, rho24, gr, grw, nv, ng, k):
+    rho24 = np.asarray(rho24, dtype=np.float64).reshape(nv, ng)
+    rho13 = np.asarray(rho13, dtype=np.float64).reshape(nv, ng)
+    y = yk_row(rho24, gr, grw, nv, ng, k).reshape(nv, ng)
+    return float(np.sum(grw * rho13 * y))
+
+
+def _disjoint_cells(rho13, rho24, r, w, k, ng):
+    """Product rule over cell pairs (m < m'), both orderings, vectorised."""
+    n = r.shape[0]
+    cell = np.arange(n) // ng
+    later = cell[None, :] > cell[:, None]
+    with np.errstate(over="ignore", under="ignore", invalid="ignore"):
+        ker = np.where(later, (r[:, None] / r[None, :]) ** k / r[None, :], 0.0)
+    prod = w[:, None] * w[None, :] * ker * (rho13[:, None] * rho24[None, :] + rho13[None, :] * rho24[:, None])
+    return float(np.sum(prod))
+
+
+@lru_cache(maxsize=16)
+def _triangle_rule(ng, order):
+    nodes, _ = np.polynomial.legendre.leggauss(ng)
+    x, wt = np.polynomial.legendre.leggauss(order)
+    x, wt = (x + 1.0) / 2.0, wt / 2.0
+    inv = np.linalg.solve(np.polynomial.legendre.legvander(nodes, ng - 1), np.eye(ng))
+    outer = np.polynomial.legendre.legvander(2 * x - 1, ng - 1) @ inv
+    inner = np.polynomial.legendre.legvander(2 * x[:, None] * x[None, :] - 1, ng - 1) @ inv
+    return nodes, x, wt, outer, inner
+
+
+def slater_rk_direct(rho13, rho24, gr, grw, k):
+    """O(N^2) double quadrature with each coincident cell split along r = s.
+
+    Disjoint cell pairs use the tensor Gauss rule; a coincident cell uses the
+    Duffy-type map r = a + h x, s = a + h x y on its lower triangle with a
+    Gauss rule of order max(2 ng, (k + ng + 1)//2) in both x and y and the
+    densities taken from their node interpolants.
+    """
+    gr, grw = np.asarray(gr, dtype=np.float64), np.asarray(grw, dtype=np.float64)
+    nv, ng = gr.shape
+    rho13 = np.asarray(rho13, dtype=np.float64).reshape(nv, ng)
+    rho24 = np.asarray(rho24, dtype=np.float64).reshape(nv, ng)
+    off = _disjoint_cells(rho13.ravel(), rho24.ravel(), gr.ravel(), grw.ravel(), k, ng)
+    order = max(2 * ng, (k + ng + 1) // 2)
+    nodes, x, wt, outer, inner = _triangle_rule(ng, order)
+    h = grw.sum(axis=1)
+    a = gr[:, 0] - h * (1 + nodes[0]) / 2
+    r = a[:, None, None] + h[:, None, None] * x[None, :, None]
+    s = a[:, None, None] + h[:, None, None] * x[None, :, None] * x[None, None, :]
+    kj = (s / r) ** k / r * h[:, None, None] ** 2 * x[None, :, None]
+    fo, go = rho13 @ outer.T, rho24 @ outer.T
+    fi = np.einsum("cj,xyj->cxy", rho13, inner)
+    gi = np.einsum("cj,xyj->cxy", rho24, inner)
+    dens = fo[:, :, None] * gi + go[:, :, None] * fi
+    diag = float(np.sum(dens * kj * wt[None, :, None] * wt[None, None, :]))
+    return off + diag
