@@ -1,0 +1,740 @@
+// Split-precision R^k engine: factored Green operator + Ozaki-II (CRT) INT8
+// residue GEMMs on the 5th-generation tensor cores, recombined in FP64.
+//
+//   R(ac;bd) = X_ac . X_bd - Z_ac . Z_bd + left_ac . right_bd
+//
+// K2x  split_rows_kernel  (one warp per (pair, k) row, FP64 on CUDA cores)
+//      g = w (P_a P_c + Q_a Q_c);  per body cell m >= 1:  d_m = u_m . g_m and
+//      the exclusive suffix sums T_m = sum_{m'>m} d_m' (warp-shuffle scans);
+//      X_m = L_mm^T g_m + c_m T_m + ell_m (v_0.g_0);  Z_e = z_e . g_{cell(e)};
+//      FP64 core terms left = g_0, right = S_c g_0 (core Schur complement).
+//      Each row [X | Z] is scaled by a power of two to |x| < 2^bits, rounded
+//      to an integer x~ and written as int8 residues x~ mod m_i (and the B copy
+//      with Z negated) in a [modulus][row][kpad] layout.
+//
+// K3s  crt_syrk_kernel  (persistent, one CTA per SM, 10 warps)
+//      warp 0: TMA producer — 128x128-byte boxes (SWIZZLE_128B) of the A and B
+//              residue matrices into a STAGES-deep ring;
+//      warp 1: TMEM owner + MMA issuer — tcgen05.mma.kind::i8, M=N=128, K=32,
+//              int32 accumulators in a double-buffered TMEM tile;
+//      warps 2-9: epilogue (4 TMEM lane quarters x 2 column halves) — per
+//              modulus: TMEM -> registers, reduce mod m_i, pack 4 residues per
+//              32-bit word (groups of 4 moduli parked in TMEM columns 256..511,
+//              the last group kept in registers); per tile: CRT in FP64 (exact
+//              split constants), scale, add the core correction, store the
+//              tile and its transpose.
+//      Every mbarrier wait is bounded; on timeout the kernel records
+//      RKB_ETIMEDOUT in *status and every role drains and returns.
+#include <cuda.h>
+
+#include "rkb_common.cuh"
+
+namespace rkb {
+namespace split {
+
+constexpr int MAXMOD = 12;
+
+// =========================================================================
+// K2x — transform, quantise, residues
+// =========================================================================
+struct RowsArgs {
+    const double *P, *Q;
+    long orb_ld;
+    const long *pairs, *row_pair;
+    const int *row_k;
+    long nrows;
+    const double *w;
+    int nv, ng;
+    const double *ktab;
+    const long *koff;  // by k
+    int bits, n_mod;
+    int mod[MAXMOD];
+    double inv_mod[MAXMOD];
+    signed char *resA, *resB;  // [n_mod][nrows_total][kpad]; resB may be null
+    long kpad, row_base, nrows_total;
+    double *rowscale, *left, *right, *cbound;
+    int cwp;
+};
+
+__device__ __forceinline__ double rho_at(const RowsArgs &a, long q, long i) {
+    long p = a.row_pair[q];
+    long x = a.pairs[2 * p], c = a.pairs[2 * p + 1];
+    return __dadd_rn(__dmul_rn(a.P[x * a.orb_ld + i], a.P[c * a.orb_ld + i]),
+                     __dmul_rn(a.Q[x * a.orb_ld + i], a.Q[c * a.orb_ld + i]));
+}
+
+// x in (-2^bits, 2^bits) integer-valued double -> residue in [-128, 127]
+__device__ __forceinline__ int residue_of(double x, int m, double inv_m) {
+    double q = rint(x * inv_m);
+    int r = (int)fma(-q, (double)m, x);
+    if (r > 127) r -= m;
+    if (r < -128) r += m;
+    return r;
+}
+
+template <int NG>
+__global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
+    constexpr int NGMAX = NG > 0 ? NG : RKB_MAX_NG;
+    const int ng = NG > 0 ? NG : a.ng;
+    const int nv = a.nv;
+    const long n = (long)nv * ng;
+    extern __shared__ double sm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *g = sm + (long)wib * (n + nv);
+    double *tsuf = g + n;  // exclusive suffix sums per cell
+    const long q = (long)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (q >= a.nrows) return;
+    const int k = a.row_k[q];
+    const double *tab = a.ktab + a.koff[k];
+    const double *u = tab;
+    const double *ell = u + n;
+    const double *Lb = ell + n;
+    const double *C = Lb + (long)nv * ng * ng;
+    const double *v0 = C + (long)nv * ng;
+    const double *Sc = v0 + ng;
+    const int nz = (int)Sc[ng * ng];
+    const double *zt = Sc + ng * ng + 1;
+    const long kbody = (long)(nv - 1) * ng;
+
+    for (long i = lane; i < n; i += 32) g[i] = __dmul_rn(a.w[i], rho_at(a, q, i));
+    __syncwarp();
+    // alpha = v_0 . g_0: the core charge moment that couples into every X
+    double alpha = 0.0;
+    for (int j = lane; j < ng; j += 32) alpha = fma(v0[j], g[j], alpha);
+    alpha = warp_sum(alpha);
+
+    // suffix sums over body cells (cell 0 contributes nothing)
+    const int nch = (nv + 31) >> 5;
+    double carry = 0.0;
+    for (int c = 0; c < nch; ++c) {
+        int m = nv - 1 - ((c << 5) + lane);
+        double d = 0.0;
+        if (m >= 1) {
+            for (int j = 0; j < ng; ++j) d = fma(u[(long)m * ng + j], g[(long)m * ng + j], d);
+        }
+        double incl = warp_inclusive_scan(d, lane);
+        double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (m >= 0) tsuf[m] = lane == 0 ? carry : carry + excl;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+
+    // pass A: row maximum of |[X | Z]|
+    double amax = 0.0;
+    for (int m = 1 + lane; m < nv; m += 32) {
+        const double *L = Lb + (long)m * ng * ng;
+        const double *gm = g + (long)m * ng;
+        double t = tsuf[m];
+#pragma unroll
+        for (int j = 0; j < NGMAX; ++j) {
+            if (j < ng) {
+                double x = fma(ell[(long)m * ng + j], alpha, C[(long)m * ng + j] * t);
+                for (int i = j; i < ng; ++i) x = fma(L[i * ng + j], gm[i], x);
+                amax = fmax(amax, fabs(x));
+            }
+        }
+    }
+    for (int e = lane; e < nz; e += 32) {
+        const double *ze = zt + (long)e * (ng + 1);
+        const double *gm = g + (long)ze[0] * ng;
+        double x = 0.0;
+        for (int i = 0; i < ng; ++i) x = fma(ze[1 + i], gm[i], x);
+        amax = fmax(amax, fabs(x));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+
+    int ex = 0;
+    double scale = 0.0, inv_scale = 0.0;
+    if (amax > 0.0 && isfinite(amax)) {
+        frexp(amax, &ex);  // amax < 2^ex
+        scale = ldexp(1.0, a.bits - ex);
+        inv_scale = ldexp(1.0, ex - a.bits);
+    }
+    const long grow = a.row_base + q;  // row index in the residue matrices
+
+    // pass B: quantise and write residues (lane = cell -> ng contiguous bytes)
+    for (int m = 1 + lane; m < nv; m += 32) {
+        const double *L = Lb + (long)m * ng * ng;
+        const double *gm = g + (long)m * ng;
+        double t = tsuf[m];
+        double xq[NGMAX];
+#pragma unroll
+        for (int j = 0; j < NGMAX; ++j) {
+            if (j < ng) {
+                double x = fma(ell[(long)m * ng + j], alpha, C[(long)m * ng + j] * t);
+                for (int i = j; i < ng; ++i) x = fma(L[i * ng + j], gm[i], x);
+                xq[j] = rint(x * scale);
+            }
+        }
+        const long col = (long)(m - 1) * ng;
+        for (int md = 0; md < a.n_mod; ++md) {
+            signed char *dA = a.resA + ((long)md * a.nrows_total + grow) * a.kpad + col;
+            signed char *dB = a.resB ? a.resB + ((long)md * a.nrows_total + grow) * a.kpad + col : nullptr;
+#pragma unroll
+            for (int j = 0; j < NGMAX; ++j) {
+                if (j < ng) {
+                    signed char r = (signed char)residue_of(xq[j], a.mod[md], a.inv_mod[md]);
+                    dA[j] = r;
+                    if (dB) dB[j] = r;
+                }
+            }
+        }
+    }
+    for (int e = lane; e < nz; e += 32) {
+        const double *ze = zt + (long)e * (ng + 1);
+        const double *gm = g + (long)ze[0] * ng;
+        double x = 0.0;
+        for (int i = 0; i < ng; ++i) x = fma(ze[1 + i], gm[i], x);
+        double xq = rint(x * scale);
+        for (int md = 0; md < a.n_mod; ++md) {
+            long o = ((long)md * a.nrows_total + grow) * a.kpad + kbody + e;
+            int r = residue_of(xq, a.mod[md], a.inv_mod[md]);
+            a.resA[o] = (signed char)r;
+            if (a.resB) a.resB[o] = (signed char)residue_of(-xq, a.mod[md], a.inv_mod[md]);
+        }
+    }
+    // zero padding columns
+    for (long c = kbody + nz + lane; c < a.kpad; c += 32) {
+        for (int md = 0; md < a.n_mod; ++md) {
+            long o = ((long)md * a.nrows_total + grow) * a.kpad + c;
+            a.resA[o] = 0;
+            if (a.resB) a.resB[o] = 0;
+        }
+    }
+    // FP64 core correction: left = g_0, right = S_c g_0, and the screen bounds
+    double *lf = a.left + grow * a.cwp, *rt = a.right + grow * a.cwp;
+    double n1 = 0.0, n2 = 0.0;
+    for (int i = lane; i < a.cwp; i += 32) {
+        double gi = 0.0, s = 0.0;
+        if (i < ng) {
+            gi = g[i];
+            for (int j = 0; j < ng; ++j) s = fma(Sc[i * ng + j], g[j], s);
+        }
+        lf[i] = gi;
+        rt[i] = s;
+        n1 = fma(gi, gi, n1);
+        n2 = fma(s, s, n2);
+    }
+    n1 = warp_sum(n1);
+    n2 = warp_sum(n2);
+    if (lane == 0) {
+        a.rowscale[grow] = inv_scale;
+        // bounds of |g_0| and |S_c g_0| relative to 2^ex (>= the row maximum of
+        // |[X | Z]|); a zero row keeps them infinite (never screened)
+        const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
+        a.cbound[grow * 2] = sqrt(n1) * rel;
+        a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+    }
+}
+
+// =========================================================================
+// K3s — tcgen05 INT8 residue SYRK with CRT epilogue
+// =========================================================================
+constexpr int BM = 128, BN = 128, BKB = 128;  // tile rows, tile cols, K bytes per stage
+constexpr int STAGES = 5;
+constexpr int STAGE_BYTES = (BM + BN) * BKB;  // 32 KB
+constexpr int EPI_WARPS = 8;                  // 4 TMEM lane quarters x 2 column halves
+constexpr int EPI_COLS = BN / 2;              // columns per epilogue thread
+constexpr int THREADS = 32 * (2 + EPI_WARPS);
+constexpr int STG_LD = 17;  // doubles per staged row (16 + pad)
+constexpr size_t SMEM_BYTES = 1024 /*align slack*/ + (size_t)STAGES * STAGE_BYTES +
+                              (size_t)EPI_WARPS * 32 * STG_LD * sizeof(double) + 256 /*barriers*/;
+constexpr long long WAIT_LIMIT = 4000000000LL;  // clock64 ticks (~2 s)
+constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+struct CrtArgs {
+    const double *rowscale, *left, *right, *cbound;
+    double corr_floor;  // skip the FP64 core correction of a warp block when its bound is below this
+    int cwp, cw;
+    const long *grp_row0, *grp_n, *grp_kdim, *grp_out;
+    const int *tasks;
+    long n_tasks, nrows_total;
+    double *out;
+    int *status;
+    int n_mod;
+    int mod[MAXMOD];
+    float inv_mod[MAXMOD];
+    double f_hi[MAXMOD], f_lo[MAXMOD];
+    double M;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false (and status = ETIMEDOUT) after WAIT_LIMIT clock ticks,
+// or as soon as another role has recorded a failure.
+__device__ __forceinline__ bool mbar_wait_slow(uint64_t *bar, uint32_t parity, int *status) {
+    long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (*(volatile int *)status != 0) return false;
+        if (clock64() - t0 > WAIT_LIMIT) {
+            atomicExch(status, (int)RKB_ETIMEDOUT);
+            return false;
+        }
+    }
+    return true;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *status) {
+    if (mbar_try(bar, parity)) return true;
+    return mbar_wait_slow(bar, parity, status);
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);   // start address (16-byte units)
+    d |= (uint64_t)1u << 16;                   // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024u >> 4) << 32;         // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1u << 46;                   // descriptor version for sm_100
+    d |= (uint64_t)2u << 61;                   // SWIZZLE_128B
+    return d;
+}
+__device__ __forceinline__ void mma_i8(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+        "l"(ad), "l"(bd), "r"(IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t *v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::
+            "r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// int32 accumulator -> a representative of v mod m in [-128, 127].  The
+// float quotient is off by at most one for |v| < 2^25, which one conditional
+// add and one conditional subtract absorb.
+__device__ __forceinline__ uint32_t residue_byte(int v, int m, float inv_m) {
+    int q = __float2int_rn(__int2float_rn(v) * inv_m);
+    int r = v - q * m;
+    r += (r < -128) ? m : 0;
+    r -= (r > 127) ? m : 0;
+    return (uint32_t)r & 0xffu;
+}
+
+template <int NMOD>
+__global__ void __launch_bounds__(THREADS, 1)
+    crt_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                    const __grid_constant__ CrtArgs p) {
+    constexpr int PARKED = (NMOD - 1) >> 2;  // groups of four moduli parked in TMEM (0..2)
+    constexpr int LASTG = PARKED;            // group kept in registers
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char *ring = base;
+    double *stage_out = (double *)(ring + (size_t)STAGES * STAGE_BYTES);
+    uint64_t *bars = (uint64_t *)(stage_out + EPI_WARPS * 32 * STG_LD);
+    uint64_t *full = bars, *empty = bars + STAGES, *accf = bars + 2 * STAGES, *acce = accf + 2;
+    uint32_t *tmem_slot = (uint32_t *)(acce + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], EPI_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    int *status = p.status;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (long t = blockIdx.x; t < p.n_tasks && ok; t += gridDim.x) {
+                const int g = p.tasks[3 * t], ti = p.tasks[3 * t + 1], tj = p.tasks[3 * t + 2];
+                const long row0 = p.grp_row0[g];
+                const int nk = (int)(p.grp_kdim[g] / BKB);
+                for (int md = 0; md < NMOD && ok; ++md) {
+                    const int ya = (int)(md * p.nrows_total + row0 + (long)ti * BM);
+                    const int yb = (int)(md * p.nrows_total + row0 + (long)tj * BN);
+                    for (int kc = 0; kc < nk; ++kc, ++it) {
+                        const int s = it % STAGES;
+                        const uint32_t ph = (it / STAGES) & 1u;
+                        if (!mbar_wait(&empty[s], ph ^ 1u, status)) { ok = false; break; }
+                        unsigned char *sa = ring + (size_t)s * STAGE_BYTES;
+                        mbar_expect_tx(&full[s], STAGE_BYTES);
+                        tma_load(sa, &mapA, kc * BKB, ya, &full[s]);
+                        tma_load(sa + BM * BKB, &mapB, kc * BKB, yb, &full[s]);
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            uint32_t it = 0, acc_it = 0;
+            bool ok = true;
+            for (long t = blockIdx.x; t < p.n_tasks && ok; t += gridDim.x) {
+                const int g = p.tasks[3 * t];
+                const int nk = (int)(p.grp_kdim[g] / BKB);
+                for (int md = 0; md < NMOD && ok; ++md, ++acc_it) {
+                    const int buf = acc_it & 1;
+                    const uint32_t aph = (acc_it >> 1) & 1u;
+                    if (!mbar_wait(&acce[buf], aph ^ 1u, status)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t dt = tmem + (uint32_t)(buf * BN);
+                    for (int kc = 0; kc < nk; ++kc, ++it) {
+                        const int s = it % STAGES;
+                        const uint32_t ph = (it / STAGES) & 1u;
+                        if (!mbar_wait(&full[s], ph, status)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t sa = smem_u32(ring + (size_t)s * STAGE_BYTES);
+                        const uint64_t ad = sw128_desc(sa), bd = sw128_desc(sa + BM * BKB);
+#pragma unroll
+                        for (int kk = 0; kk < BKB / 32; ++kk)
+                            mma_i8(dt, ad + (uint64_t)(2 * kk), bd + (uint64_t)(2 * kk), (kc | kk) != 0 ? 1u : 0u);
+                        mma_commit(&empty[s]);
+                    }
+                    if (ok) mma_commit(&accf[buf]);
+                }
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int ew = warp - 2;
+        const int quarter = warp & 3;       // TMEM lane quarter this warp may access
+        const int half = ew >> 2;           // column half of the tile
+        const int rloc = quarter * 32 + lane;
+        const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
+        const uint32_t col0 = (uint32_t)(half * EPI_COLS);
+        double *stg = stage_out + (size_t)ew * 32 * STG_LD;
+        uint32_t acc_it = 0;
+        bool ok = true;
+        for (long t = blockIdx.x; t < p.n_tasks && ok; t += gridDim.x) {
+            const int g = p.tasks[3 * t], ti = p.tasks[3 * t + 1], tj = p.tasks[3 * t + 2];
+            const long row0 = p.grp_row0[g], n = p.grp_n[g];
+            const long a = (long)ti * BM + rloc;  // table row of this thread
+            const long b0 = (long)tj * BN + col0;
+            uint32_t pk[EPI_COLS];
+#pragma unroll
+            for (int c = 0; c < EPI_COLS; ++c) pk[c] = 0u;
+#pragma unroll 1
+            for (int md = 0; md < NMOD; ++md, ++acc_it) {
+                const int buf = acc_it & 1;
+                const uint32_t aph = (acc_it >> 1) & 1u;
+                if (!mbar_wait(&accf[buf], aph, status)) { ok = false; break; }
+                tc_fence_after();
+                const int m = p.mod[md];
+                const float im = p.inv_mod[md];
+#pragma unroll
+                for (int c = 0; c < EPI_COLS / 16; ++c) {
+                    uint32_t v[16];
+                    tmem_ld16(tmem + lane_off + (uint32_t)(buf * BN) + col0 + (uint32_t)(c * 16), v);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) pk[c * 16 + j] |= residue_byte((int)v[j], m, im) << (8 * (md & 3));
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acce[buf]);
+                if ((md & 3) == 3 && (md >> 2) < PARKED) {
+                    // park a completed group of four moduli in TMEM columns 256 + 128*group
+                    const uint32_t col = 256u + 128u * (uint32_t)(md >> 2) + col0;
+#pragma unroll
+                    for (int c = 0; c < EPI_COLS / 16; ++c) tmem_st16(tmem + lane_off + col + (uint32_t)(c * 16), &pk[c * 16]);
+                    tmem_wait_st();
+#pragma unroll
+                    for (int c = 0; c < EPI_COLS; ++c) pk[c] = 0u;
+                }
+            }
+            if (!ok) break;
+            // ---- CRT, scaling, correction and stores
+            const bool arow = a < n;
+            const double rs_a = arow ? __ldg(p.rowscale + row0 + a) : 0.0;
+            const double *la = p.left + (row0 + (arow ? a : 0)) * p.cwp;
+            const bool mirror = ti != tj;
+            double *R = p.out + p.grp_out[g];
+            // Correction screen for this warp's 32 x 64 block: with per-row bounds
+            // relative to each row's scale, |left_a . right_b| <= 2^(e_a+e_b) *
+            // |g0_a| |S_c g0_b|.  Below corr_floor the term is far under the
+            // split's own error and is skipped.
+            double r1 = 0.0, c2 = 0.0;
+            if (arow) r1 = __ldg(p.cbound + (row0 + a) * 2);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const long bcol = b0 + lane + 32 * h;
+                if (bcol < n) c2 = fmax(c2, __ldg(p.cbound + (row0 + bcol) * 2 + 1));
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                r1 = fmax(r1, __shfl_xor_sync(0xffffffffu, r1, o));
+                c2 = fmax(c2, __shfl_xor_sync(0xffffffffu, c2, o));
+            }
+            const bool need_corr = !(r1 * c2 <= p.corr_floor);
+            constexpr int FC = 8;  // columns per final-phase chunk
+#pragma unroll
+            for (int c = 0; c < EPI_COLS / FC; ++c) {
+                uint32_t w0[FC], w1[FC];
+                if (PARKED >= 1) tmem_ld8(tmem + lane_off + 256u + col0 + (uint32_t)(c * FC), w0);
+                if (PARKED >= 2) tmem_ld8(tmem + lane_off + 384u + col0 + (uint32_t)(c * FC), w1);
+                tmem_wait_ld();
+                double xs[FC];
+#pragma unroll
+                for (int j = 0; j < FC; ++j) {
+                    double yh = 0.0, yl = 0.0;
+#pragma unroll
+                    for (int md = 0; md < NMOD; ++md) {
+                        const int grp = md >> 2;
+                        const uint32_t word = grp == LASTG ? pk[c * FC + j] : (grp == 0 ? w0[j] : w1[j]);
+                        const double r = (double)(int)(signed char)(word >> (8 * (md & 3)));
+                        yh = fma(r, p.f_hi[md], yh);
+                        yl = fma(r, p.f_lo[md], yl);
+                    }
+                    const long b = b0 + c * FC + j;
+                    const double rs_b = b < n ? __ldg(p.rowscale + row0 + b) : 0.0;
+                    xs[j] = ((yh - rint(yh)) * p.M + yl * p.M) * (rs_a * rs_b);
+                }
+                if (need_corr && arow) {  // warp-uniform except for the row guard
+                    for (int j = 0; j < FC; ++j) {
+                        const long b = b0 + c * FC + j;
+                        if (b < n) {
+                            const double *rb = p.right + (row0 + b) * p.cwp;
+                            double corr = 0.0;
+                            for (int i = 0; i < p.cw; ++i) corr = fma(__ldg(la + i), __ldg(rb + i), corr);
+                            xs[j] += corr;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < FC; ++j) {
+                    const long b = b0 + c * FC + j;
+                    const bool valid = arow && b < n;
+                    const double v = valid ? xs[j] : 0.0;
+                    if (valid) {
+                        if (!isfinite(v)) atomicExch(status, (int)RKB_ENONFINITE);
+                        if (mirror) R[b * n + a] = v;  // lanes hold consecutive a: coalesced
+                    }
+                    stg[lane * STG_LD + (c & 1) * FC + j] = v;
+                }
+                if (c & 1) {
+                    // direct tile row segment of 16 columns through shared memory (coalesced rows)
+                    __syncwarp();
+                    const long a0 = (long)ti * BM + quarter * 32;
+                    const long bc = b0 + (c - 1) * FC;
+#pragma unroll 4
+                    for (int rr = 0; rr < 32; rr += 2) {
+                        const int row = rr + (lane >> 4), col = lane & 15;
+                        const long aa = a0 + row, bb = bc + col;
+                        if (aa < n && bb < n) R[aa * n + bb] = stg[row * STG_LD + col];
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// ------------------------------------------------------------- host helpers
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)f;
+    }
+    return fn;
+}
+
+static int make_map(CUtensorMap *map, const void *ptr, long kpad, long rows) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled is unavailable from the CUDA driver");
+        return RKB_EUNSUPPORTED;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kpad};
+    cuuint32_t box[2] = {(cuuint32_t)BKB, (cuuint32_t)BM};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void *>(ptr), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d) for a %ld x %ld residue matrix", (int)r, rows, kpad);
+        return RKB_EINVAL;
+    }
+    return RKB_OK;
+}
+
+}  // namespace split
+}  // namespace rkb
+
+using namespace rkb;
+using namespace rkb::split;
+
+extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                              const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w, int nv,
+                              int ng, const double *d_ktab, const long *d_koff, int bits, int n_mod,
+                              const int *moduli, signed char *d_resA, signed char *d_resB, long kpad,
+                              long row_base, long nrows_total, double *d_rowscale, double *d_left,
+                              double *d_right, double *d_cbound, int cwp, void *stream) {
+    RKB_CHECK_ARG(nv >= 2 && ng >= 1 && ng <= RKB_MAX_NG, "invalid grid (nv=%d, ng=%d)", nv, ng);
+    RKB_CHECK_ARG(bits >= 8 && bits <= 50, "bits must be in [8, 50] (got %d)", bits);
+    RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
+    RKB_CHECK_ARG(kpad % BKB == 0 && kpad >= (long)(nv - 1) * ng, "kpad must be a multiple of %d >= body width",
+                  BKB);
+    RKB_CHECK_ARG(cwp >= ng, "correction width must be >= ng");
+    RKB_CHECK_ARG(d_cbound != nullptr, "the correction-bound array is required");
+    RKB_CHECK_ARG(row_base >= 0 && row_base + nrows <= nrows_total, "row range outside the residue matrices");
+    if (nrows == 0) return RKB_OK;
+    RowsArgs a;
+    a.P = d_Pv; a.Q = d_Qv; a.orb_ld = orb_ld; a.pairs = d_pairs; a.row_pair = d_row_pair; a.row_k = d_row_k;
+    a.nrows = nrows; a.w = d_w; a.nv = nv; a.ng = ng; a.ktab = d_ktab; a.koff = d_koff; a.bits = bits;
+    a.n_mod = n_mod;
+    for (int i = 0; i < MAXMOD; ++i) {
+        a.mod[i] = i < n_mod ? moduli[i] : 1;
+        a.inv_mod[i] = 1.0 / (double)a.mod[i];
+    }
+    a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
+    a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
+    const int warps = 4;
+    size_t smem = (size_t)warps * ((long)nv * ng + nv) * sizeof(double);
+    RKB_CHECK_ARG(smem <= 200 * 1024, "grid too large for the split row kernel");
+    dim3 grid((unsigned)ceil_div(nrows, warps)), block(32 * warps);
+    cudaStream_t st = as_stream(stream);
+#define RKB_SR_CASE(NGV)                                                                              \
+    case NGV: {                                                                                       \
+        RKB_CUDA(cudaFuncSetAttribute(split_rows_kernel<NGV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                      (int)smem));                                                    \
+        split_rows_kernel<NGV><<<grid, block, smem, st>>>(a);                                         \
+        break;                                                                                        \
+    }
+    switch (ng) {
+        RKB_SR_CASE(5) RKB_SR_CASE(7) RKB_SR_CASE(8) RKB_SR_CASE(9) RKB_SR_CASE(11)
+        default: {
+            RKB_CUDA(cudaFuncSetAttribute(split_rows_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            split_rows_kernel<0><<<grid, block, smem, st>>>(a);
+        }
+    }
+#undef RKB_SR_CASE
+    RKB_LAUNCHED("split_rows_kernel");
+    return RKB_OK;
+}
+
+extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, long kpad,
+                                  long nrows_total, int n_mod, const int *moduli, const double *f_hi,
+                                  const double *f_lo, double M, const double *d_rowscale, const double *d_left,
+                                  const double *d_right, const double *d_cbound, double corr_floor, int cw,
+                                  int cwp, const long *d_grp_row0,
+                                  const long *d_grp_n, const long *d_grp_kdim, const long *d_grp_out,
+                                  const int *d_tasks, long n_tasks, double *d_out, int *d_status, void *stream) {
+    RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
+    RKB_CHECK_ARG(kpad % BKB == 0 && kpad > 0, "kpad must be a positive multiple of %d", BKB);
+    RKB_CHECK_ARG((long)n_mod * nrows_total < (1L << 31), "residue matrices too tall for 32-bit TMA rows");
+    RKB_CHECK_ARG(d_status != nullptr, "a device status word is required");
+    RKB_CHECK_ARG(cw <= cwp, "cw must be <= cwp");
+    RKB_CHECK_ARG(d_cbound != nullptr && corr_floor >= 0.0, "correction bounds and a nonnegative floor are required");
+    if (n_tasks == 0) return RKB_OK;
+    CUtensorMap mA, mB;
+    int rc = make_map(&mA, d_resA, kpad, (long)n_mod * nrows_total);
+    if (rc) return rc;
+    rc = make_map(&mB, d_resB ? d_resB : d_resA, kpad, (long)n_mod * nrows_total);
+    if (rc) return rc;
+    CrtArgs p;
+    p.rowscale = d_rowscale; p.left = d_left; p.right = d_right; p.cbound = d_cbound; p.corr_floor = corr_floor;
+    p.cwp = cwp; p.cw = cw;
+    p.grp_row0 = d_grp_row0; p.grp_n = d_grp_n; p.grp_kdim = d_grp_kdim; p.grp_out = d_grp_out;
+    p.tasks = d_tasks; p.n_tasks = n_tasks; p.nrows_total = nrows_total; p.out = d_out; p.status = d_status;
+    p.n_mod = n_mod; p.M = M;
+    for (int i = 0; i < MAXMOD; ++i) {
+        p.mod[i] = i < n_mod ? moduli[i] : 1;
+        p.inv_mod[i] = 1.0f / (float)p.mod[i];
+        p.f_hi[i] = i < n_mod ? f_hi[i] : 0.0;
+        p.f_lo[i] = i < n_mod ? f_lo[i] : 0.0;
+    }
+    long grid = n_tasks < sm_count() ? n_tasks : sm_count();
+    cudaStream_t st = as_stream(stream);
+#define RKB_CRT_CASE(NM)                                                                                     \
+    case NM: {                                                                                               \
+        RKB_CUDA(cudaFuncSetAttribute(crt_syrk_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                      (int)SMEM_BYTES));                                                     \
+        crt_syrk_kernel<NM><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(mA, mB, p);                         \
+        break;                                                                                               \
+    }
+    switch (n_mod) {
+        RKB_CRT_CASE(4) RKB_CRT_CASE(5) RKB_CRT_CASE(6) RKB_CRT_CASE(7) RKB_CRT_CASE(8) RKB_CRT_CASE(9)
+        RKB_CRT_CASE(10) RKB_CRT_CASE(11) RKB_CRT_CASE(12)
+        default:
+            set_error("split contraction compiled for 4..12 moduli (got %d)", n_mod);
+            return RKB_EINVAL;
+    }
+#undef RKB_CRT_CASE
+    RKB_LAUNCHED("crt_syrk_kernel");
+    return RKB_OK;
+}

@@ -1,0 +1,163 @@
+"""Host planning for the split-precision (Ozaki-II / CRT) R^k engine.
+
+Factored Green operator
+-----------------------
+With g = w*rho on the cell Gauss grid, atomx's R^k(ac;bd) = g_ac^T G g_bd
+(numerics/yk.py:88-154 builds Y = G g; numerics/bspline/slater.py:130
+contracts it).  G is symmetric: its off-cell blocks are the exact kernel
+samples r_<^k / r_>^{k+1}, and inside a cell the interpolatory partial
+matrices satisfy mo + mo^T = 1, so G_ij = u_i v_j mo_ij + v_i u_j mo_ji with
+u = r^-(k+1), v = r^k.  Off-diagonal cell blocks are rank one, so G is
+block-semiseparable.
+
+Split G at cell 0 (the cell [0, r_min] whose partial rule acts on an
+endpoint-singular integrand and whose block is violently indefinite) and
+eliminate the body first, the core last:
+
+  R = X_ac . X_bd - Z_ac . Z_bd + left_ac . right_bd
+
+* body (cells >= 1): a block Cholesky of the semiseparable G_bb computed by
+  the recursion  S_m = D_m - sigma_m u_m u_m^T,  L_mm L_mm^T = S_m + Delta_m,
+  c_m = L_mm^{-1} (v_m - sigma_m u_m),  sigma_{m+1} = sigma_m + |c_m|^2,
+  which gives X = L^T g per row in O(N ng):
+      X_m = L_mm^T g_m + c_m * sum_{m' > m} u_m'.g_m'.
+  Delta_m (a modified-Cholesky shift, rank = number of Schur eigenvalues
+  below tau * lambda_max of the diagonally scaled block) is returned as
+  extra columns Z with a negative sign: g^T Delta g = sum_e (z_e . g_m)^2;
+* the core-body coupling G_cb = v_0 u_b^T is rank one and moves into X:
+  with ell = L^-1 u_b (block forward substitution,
+  L_mm ell_m = u_m (1 - sum_{m'<m} c_m'.ell_m')),
+      X = L^T g_b + ell * (v_0 . g_0),
+  which reproduces both cross terms (ell . L^T g = u_b . g);
+* what is left is the core Schur complement S_c = G_00 - |ell|^2 v_0 v_0^T,
+  kept in FP64: left = g_0, right = S_c g_0.  For physical densities it is
+  many orders below the entries (cell 0 holds almost no charge).
+
+|X_ac.X_bd| <= |X_ac||X_bd| = sqrt(R_acac R_bdbd) (up to the small Delta),
+so a per-row fixed-point split of X has an error bounded relative to the
+Schwarz scale of every entry, which is what the split engine needs.
+
+CRT constants
+-------------
+Pairwise-coprime moduli m_i <= 256 (int8 residues in [-128, 127]), M = prod m_i.
+An integer x with |x| < M/2 is rebuilt from residues r_i as
+x = M * frac(sum_i r_i f_i), f_i = (M/m_i) [(M/m_i)^-1 mod m_i] / M mod 1.
+f_i is split into f_hi (a multiple of 2^-42) and f_lo = f_i - f_hi so that
+sum r_i f_hi is exact in one double for |r_i| <= 128 and up to 12 moduli.
+"""
+from __future__ import annotations
+
+import math
+from fractions import Fraction
+from functools import lru_cache
+
+import numpy as np
+
+from .yk import yk_partial_matrices
+
+__all__ = ["MODULI", "crt_constants", "moduli_needed", "green_factor", "pack_factors", "factor_table_layout"]
+
+#: Pairwise-coprime moduli, largest first (256 = 2^8; 255 = 3*5*17; 253 = 11*23;
+#: 247 = 13*19; 217 = 7*31; the rest are primes).
+MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217)
+MAX_MODULI = 12
+
+
+def moduli_needed(bits: int, kdim: int) -> int:
+    """Fewest leading moduli whose product exceeds 2 * kdim * 2^(2*bits) + 2."""
+    need = 2 * kdim * (1 << (2 * bits)) + 2
+    prod = 1
+    for i, m in enumerate(MODULI):
+        prod *= m
+        if prod > need:
+            return i + 1
+    raise ValueError(f"{bits}-bit splits of length {kdim} need more than {MAX_MODULI} int8 moduli")
+
+
+@lru_cache(maxsize=16)
+def crt_constants(n_mod: int):
+    """(moduli, f_hi, f_lo, M as double) for the first n_mod moduli."""
+    if not 1 <= n_mod <= MAX_MODULI:
+        raise ValueError("1..12 moduli supported")
+    ms = MODULI[:n_mod]
+    M = math.prod(ms)
+    f_hi, f_lo = [], []
+    for m in ms:
+        Mi = M // m
+        inv = pow(Mi % m, -1, m)
+        f = Fraction((Mi * inv) % M, M)
+        hi = Fraction(round(f * (1 << 42)), 1 << 42)
+        f_hi.append(float(hi))          # exact: a multiple of 2^-42 below 1
+        f_lo.append(float(f - hi))
+    return (np.asarray(ms, dtype=np.int32), np.asarray(f_hi), np.asarray(f_lo), float(M))
+
+
+def green_factor(r_flat: np.ndarray, ng: int, k: int, tau: float = 1e-3) -> dict:
+    """Structured modified Cholesky of the body Green matrix (see module doc)."""
+    r = np.asarray(r_flat, dtype=np.float64)
+    nv = r.shape[0] // ng
+    mo, mi = yk_partial_matrices(ng)
+    u = (r ** (-(k + 1))).reshape(nv, ng)
+    v = (r ** k).reshape(nv, ng)
+    Lb = np.zeros((nv, ng, ng))
+    C = np.zeros((nv, ng))
+    zcell, zvec = [], []
+    sigma = 0.0
+    for m in range(1, nv):
+        D = u[m][:, None] * v[m][None, :] * mo + v[m][:, None] * u[m][None, :] * mi
+        D = 0.5 * (D + D.T)
+        S = D - sigma * np.outer(u[m], u[m])
+        d = np.sqrt(np.abs(np.diag(D)))
+        lam, V = np.linalg.eigh(S / np.outer(d, d))
+        floor = tau * lam[-1]
+        for e in np.flatnonzero(lam < floor):
+            shift = max(abs(lam[e]), floor) - lam[e]
+            z = np.sqrt(shift) * V[:, e] * d
+            zcell.append(m)
+            zvec.append(z)
+            S = S + np.outer(z, z)
+        Lm = np.linalg.cholesky(S)
+        Lb[m] = Lm
+        C[m] = np.linalg.solve(Lm, v[m] - sigma * u[m])
+        sigma += float(C[m] @ C[m])
+    ell = np.zeros((nv, ng))
+    s_acc = 0.0
+    for m in range(1, nv):
+        ell[m] = np.linalg.solve(Lb[m], u[m] * (1.0 - s_acc))
+        s_acc += float(C[m] @ ell[m])
+    Gcc = u[0][:, None] * v[0][None, :] * mo + v[0][:, None] * u[0][None, :] * mi
+    Sc = Gcc - float(np.sum(ell * ell)) * np.outer(v[0], v[0])
+    return dict(k=k, nv=nv, ng=ng, u=u, v0=v[0].copy(), Lb=Lb, C=C, Gcc=Gcc, ell=ell, Sc=Sc,
+                zcell=np.asarray(zcell, dtype=np.int64), zvec=np.asarray(zvec).reshape(-1, ng))
+
+
+def factor_table_layout(nv: int, ng: int) -> dict:
+    """Offsets (in doubles) of the pieces of one packed factor table."""
+    n = nv * ng
+    o = {"u": 0, "ell": n, "Lb": 2 * n}
+    o["C"] = o["Lb"] + nv * ng * ng
+    o["v0"] = o["C"] + nv * ng
+    o["Sc"] = o["v0"] + ng
+    o["nz"] = o["Sc"] + ng * ng
+    o["z"] = o["nz"] + 1
+    return o
+
+
+def pack_factors(factors: list[dict]) -> tuple[np.ndarray, np.ndarray]:
+    """Concatenate per-k factor tables: returns (flat doubles, offsets by list index).
+
+    Layout of one table (doubles): u[N] | ell[N] | Lb[nv][ng][ng] | C[nv][ng] |
+    v0[ng] | Sc[ng][ng] | nZ | nZ x (cell, z[ng]).
+    """
+    parts, offs, off = [], [], 0
+    for F in factors:
+        nv, ng = F["nv"], F["ng"]
+        nz = F["zcell"].shape[0]
+        z = np.concatenate([F["zcell"].astype(np.float64)[:, None], F["zvec"]], axis=1).ravel() if nz else \
+            np.zeros(0)
+        t = np.concatenate([F["u"].ravel(), F["ell"].ravel(), F["Lb"].ravel(), F["C"].ravel(), F["v0"],
+                            F["Sc"].ravel(), [float(nz)], z])
+        offs.append(off)
+        parts.append(t)
+        off += t.shape[0]
+    return np.concatenate(parts), np.asarray(offs, dtype=np.int64)

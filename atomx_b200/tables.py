@@ -1,0 +1,219 @@
+"""Whole R^k tables of an ion on the device (batched engine).
+
+For an ion (radial basis + spinors) and k_max, ``slater_rk_tables`` returns
+every allowed R^k(ac;bd) = sum_i w_i rho_ac(r_i) Y^k[rho_bd](r_i) — the value
+atomx's ``slater_rk_poisson`` (numerics/bspline/slater.py:118) gives for each
+ordered entry — as one symmetric n_k x n_k table per multipole k over the
+pairs that allow k (``TablePlan.pairs_of_k[k]``, kappa-block ordered), in the
+shape of atomx's table API (``compute_slater_rk_table``,
+numerics/bspline/convol.py:1988).
+
+Precision forms:
+
+* ``"fp64"``  plain engine: orbital values (K1), fused density + Y^k rows
+  (K2), FP64 tensor-pipe contraction of the upper table tiles (K3).
+* ``"split"`` split engine (see ``atomx_b200.split``): factored Green operator,
+  Ozaki-II INT8 residue GEMMs on tcgen05 recombined in FP64.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native
+from .device import as_device, resident
+from .plan import TablePlan, make_plan
+from .yk import yk_partial_matrices
+
+__all__ = ["IonDevice", "RkTables", "upload_ion", "upload_values", "slater_rk_tables",
+           "slater_rk_tables_from_values", "tables_for", "tile_tasks", "TILE"]
+
+TILE = 128
+
+
+def _round_up(x: int, m: int) -> int:
+    return (x + m - 1) // m * m
+
+
+@dataclass
+class IonDevice:
+    """Device-resident inputs of one ion (basis arrays, orbital values, plan)."""
+    plan: TablePlan
+    nv: int
+    ng: int
+    n: int
+    r: torch.Tensor
+    w: torch.Tensor
+    mo: torch.Tensor
+    mi: torch.Tensor
+    Pv: torch.Tensor
+    Qv: torch.Tensor
+    pairs: torch.Tensor
+    row_pair: torch.Tensor
+    row_k: torch.Tensor
+    extra: dict = field(default_factory=dict)
+
+
+def upload_ion(ion, k_max: int | None = None, plan: TablePlan | None = None, stream=None) -> IonDevice:
+    """Copy an ion's coefficients to the device and evaluate its orbitals (K1)."""
+    L = _native.require_device()
+    bsp = ion.bsp
+    nv, ng = bsp["gr"].shape
+    n = nv * ng
+    if plan is None:
+        plan = make_plan(ion.kappa, ion.spec.k_max if k_max is None else k_max)
+    s = _native.stream_handle(stream)
+    r = resident(bsp["gr"]).reshape(-1)
+    w = resident(bsp["grw"]).reshape(-1)
+    mo_h, mi_h = yk_partial_matrices(ng)
+    mo, mi = resident(mo_h), resident(mi_h)
+    bp, bq = resident(bsp["bsp_p"]), resident(bsp["bsp_q"])
+    cp = as_device(ion.P)
+    cq = as_device(ion.Q)
+    n_orb = cp.shape[0]
+    Pv = torch.empty((n_orb, n), device=cp.device, dtype=torch.float64)
+    Qv = torch.empty_like(Pv)
+    _native.check(L.rkb_eval_orbitals(cp.data_ptr(), cp.shape[1], n_orb, bp.data_ptr(), nv, ng, bsp["ksp"],
+                                      bsp["nsp"], Pv.data_ptr(), n, s), "rkb_eval_orbitals(P)")
+    _native.check(L.rkb_eval_orbitals(cq.data_ptr(), cq.shape[1], n_orb, bq.data_ptr(), nv, ng, bsp["ksq"],
+                                      bsp["nsq"], Qv.data_ptr(), n, s), "rkb_eval_orbitals(Q)")
+    dev = cp.device
+    return IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=r, w=w, mo=mo, mi=mi, Pv=Pv, Qv=Qv,
+                     pairs=torch.as_tensor(plan.pairs.reshape(-1), device=dev),
+                     row_pair=torch.as_tensor(plan.row_pair, device=dev),
+                     row_k=torch.as_tensor(plan.row_k.astype(np.int32), device=dev),
+                     extra={"r_host": np.asarray(bsp["gr"], dtype=np.float64).reshape(-1)})
+
+
+def upload_values(Pv, Qv, kappa, gr, grw, k_max: int, plan: TablePlan | None = None) -> IonDevice:
+    """Device inputs from orbital values already on the grid (rows of Pv, Qv
+    are P_a(r_i), Q_a(r_i) on the (nv, ng) Gauss grid ``gr``/``grw``)."""
+    _native.require_device()
+    gr = np.asarray(gr) if not isinstance(gr, torch.Tensor) else gr
+    nv, ng = tuple(gr.shape)
+    n = nv * ng
+    if plan is None:
+        plan = make_plan(np.asarray(kappa), k_max)
+    mo_h, mi_h = yk_partial_matrices(ng)
+    Pd = as_device(Pv).reshape(-1, n).contiguous()
+    Qd = as_device(Qv).reshape(-1, n).contiguous()
+    dev = Pd.device
+    return IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=resident(gr).reshape(-1), w=resident(grw).reshape(-1),
+                     mo=resident(mo_h), mi=resident(mi_h), Pv=Pd, Qv=Qd,
+                     pairs=torch.as_tensor(plan.pairs.reshape(-1), device=dev),
+                     row_pair=torch.as_tensor(plan.row_pair, device=dev),
+                     row_k=torch.as_tensor(plan.row_k.astype(np.int32), device=dev),
+                     extra={"r_host": None if isinstance(gr, torch.Tensor) else np.asarray(gr, dtype=np.float64).reshape(-1)})
+
+
+def tile_tasks(sizes, tile: int = TILE):
+    """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes."""
+    out = []
+    for g, n in enumerate(sizes):
+        nt = (int(n) + tile - 1) // tile
+        for ti in range(nt):
+            for tj in range(ti, nt):
+                out.append((g, ti, tj))
+    return np.asarray(out, dtype=np.int32).reshape(-1, 3)
+
+
+@dataclass
+class RkTables:
+    """Symmetric R^k tables of one ion: ``table(k)`` is (n_k, n_k)."""
+    plan: TablePlan
+    ks: list
+    values: torch.Tensor          # concatenated row-major tables
+    offsets: dict                 # k -> start in ``values``
+    precision: str
+    info: dict = field(default_factory=dict)
+
+    def table(self, k: int) -> torch.Tensor:
+        nk = self.plan.n_of_k(k)
+        o = self.offsets[k]
+        return self.values[o:o + nk * nk].view(nk, nk)
+
+    def entry(self, k: int, ac: tuple, bd: tuple) -> float:
+        """R^k(ac;bd) by orbital indices (a <= c and b <= d not required)."""
+        pk = self.plan.pairs_of_k[k]
+        pos = {tuple(self.plan.pairs[p]): i for i, p in enumerate(pk)}
+        i = pos[tuple(sorted(ac))]
+        j = pos[tuple(sorted(bd))]
+        return float(self.table(k)[i, j].item())
+
+    def block(self, k: int, block_ac: int, block_bd: int) -> torch.Tensor:
+        """The (k, kappa-block_ac, kappa-block_bd) tile of the k-th table."""
+        ranges = {b: (s, e) for b, s, e in self.plan.block_ranges_of_k(k)}
+        (s1, e1), (s2, e2) = ranges[block_ac], ranges[block_bd]
+        return self.table(k)[s1:e1, s2:e2]
+
+    @property
+    def ordered_entries(self) -> int:
+        return self.plan.ordered_entries
+
+
+class Fp64Workspace:
+    """Device buffers of the plain engine for one ion, reusable across calls."""
+
+    def __init__(self, dev: IonDevice):
+        plan = dev.plan
+        self.ld = _round_up(dev.n, 32)
+        self.g = torch.empty((plan.n_rows, self.ld), device=dev.Pv.device, dtype=torch.float64)
+        self.y = torch.empty_like(self.g)
+        sizes = [plan.n_of_k(k) for k in plan.ks]
+        self.row0 = torch.as_tensor(np.array([plan.k_row_offset[k] for k in plan.ks], dtype=np.int64),
+                                    device=self.g.device)
+        self.nk = torch.as_tensor(np.array(sizes, dtype=np.int64), device=self.g.device)
+        offs = np.concatenate([[0], np.cumsum(np.array(sizes, dtype=np.int64) ** 2)])
+        self.out_off = torch.as_tensor(offs[:-1].astype(np.int64), device=self.g.device)
+        self.offsets = {k: int(offs[i]) for i, k in enumerate(plan.ks)}
+        self.total = int(offs[-1])
+        tasks = tile_tasks(sizes)
+        self.n_tasks = int(tasks.shape[0])
+        self.tasks = torch.as_tensor(tasks.reshape(-1), device=self.g.device)
+
+
+def run_fp64(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, stream=None) -> None:
+    """Plain FP64 engine: K2 (density + Y^k rows) then K3 (table contraction)."""
+    L = _native.load()
+    s = _native.stream_handle(stream)
+    plan = dev.plan
+    _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                        dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                        dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
+                                        dev.mi.data_ptr(), ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, s),
+                  "rkb_table_rows_fp64")
+    _native.check(L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
+                                            ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr(),
+                                            ws.n_tasks, out.data_ptr(), s), "rkb_table_contract_fp64")
+
+
+def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, **split_opts) -> RkTables:
+    """All R^k tables of one ion on the device (see module docstring)."""
+    if precision not in ("fp64", "split"):
+        raise ValueError(f"unknown precision {precision!r}; choose 'fp64' or 'split'")
+    dev = upload_ion(ion, k_max=k_max, stream=stream)
+    return tables_for(dev, precision=precision, stream=stream, **split_opts)
+
+
+def slater_rk_tables_from_values(Pv, Qv, kappa, gr, grw, k_max: int, precision: str = "fp64", stream=None,
+                                 **split_opts) -> RkTables:
+    """All R^k tables from orbital values on the grid (no B-spline stage)."""
+    if precision not in ("fp64", "split"):
+        raise ValueError(f"unknown precision {precision!r}; choose 'fp64' or 'split'")
+    dev = upload_values(Pv, Qv, kappa, gr, grw, k_max)
+    return tables_for(dev, precision=precision, stream=stream, **split_opts)
+
+
+def tables_for(dev: IonDevice, precision: str = "fp64", stream=None, **split_opts) -> RkTables:
+    if precision == "split":
+        from .split import SplitEngine
+        eng = SplitEngine(dev, **split_opts)
+        out = eng.run(stream=stream, check=True)
+        return RkTables(plan=dev.plan, ks=dev.plan.ks, values=out, offsets=eng.offsets, precision="split",
+                        info=eng.info())
+    ws = Fp64Workspace(dev)
+    out = torch.empty(ws.total, device=dev.Pv.device, dtype=torch.float64)
+    run_fp64(dev, ws, out, stream=stream)
+    return RkTables(plan=dev.plan, ks=dev.plan.ks, values=out, offsets=ws.offsets, precision="fp64")

@@ -1,0 +1,405 @@
+"""Benchmark: R^k integrals/s of whole Slater tables on B200.
+
+Workload (one step = one full table pass on one GPU): the Z=70 ion of 120
+order-9 B-splines on [1e-6, 60] bohr with 8 Gauss nodes per cell (N = 896),
+200 seeded spinors over kappa = +-1..+-7, every allowed R^k for k = 0..12
+(3.18e8 ordered entries).  Inputs are resident on the device before timing;
+the ``e2e`` leg starts from host coefficient arrays and ends with the whole
+table in pinned host memory.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--engine split|fp64]
+    python bench.py --impl reference   # the reference algorithm on host cores
+
+Multi-GPU: one process per GPU (torchrun); each rank computes its own ion
+(same workload, rank-dependent rotation seed) with no data-path collective
+(weak scaling); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "R^k integrals/s at <=1e-10 rel vs FP64: split-TC vs plain FP64; serve p50/p99"
+UNIT = "integrals/s"
+WORKLOAD = "ytterbium_scaleup: Z=70, 120 B-splines order 9, N=896, 200 spinors kappa+-1..+-7, k<=12"
+
+
+# --------------------------------------------------------------------- helpers
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    NAMES = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+             0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, index: int, period: float = 0.05):
+        self.index, self.period = index, period
+        self.samples, self.reasons = [], set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nv = None
+            return self
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for b, name in self.NAMES.items():
+                    if bits & b:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(self.period)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "MEASURED_PEAKS.json"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------- CPU baseline
+def cpu_baseline(ion, plan, budget_s: float = 12.0, threads: int = 0):
+    """Reference-algorithm port (oracle) on the host cores, on a bounded sample.
+
+    Times the two parts of the reference path separately on seeded samples:
+    Y^k rows (atomx yk_flat, one per (pair, k) row) and per-entry quadrature
+    dots (slater_rk_poisson's sum, one per ordered entry), then extrapolates
+    to the whole table: t = rows * t_row + entries * t_dot.
+    """
+    from oracle import oracle
+    bd = ion.bsp
+    gr, grw = bd["gr"], bd["grw"]
+    nv, ng = gr.shape
+    n = nv * ng
+    threads = threads or oracle.max_threads()
+    rng = np.random.default_rng(99)
+    Pg = np.array([oracle.eval_P(c, bd).ravel() for c in ion.P])
+    Qg = np.array([oracle.eval_Q(c, bd).ravel() for c in ion.Q])
+    nrow = min(plan.n_rows, 4096)
+    sel = rng.choice(plan.n_rows, size=nrow, replace=False)
+    rho = np.array([Pg[a] * Pg[c] + Qg[a] * Qg[c] for a, c in plan.pairs[plan.row_pair[sel]]])
+    ks = plan.row_k[sel]
+    t0 = time.perf_counter()
+    y = oracle.yk_rows(rho, ks, gr, grw, nv, ng, threads=threads)
+    t_rows = time.perf_counter() - t0
+    t_row = t_rows / nrow
+    g = rho * grw.reshape(1, -1)
+    # dots: grow the sample until it takes a good part of the budget
+    n_ent = 1 << 16
+    spent = t_rows
+    t_dot = None
+    while True:
+        ia = rng.integers(0, nrow, size=n_ent)
+        ib = rng.integers(0, nrow, size=n_ent)
+        t0 = time.perf_counter()
+        oracle.dot_entries(g, y, ia, ib, threads=threads)
+        dt = time.perf_counter() - t0
+        spent += dt
+        t_dot = dt / n_ent
+        if dt > budget_s / 3 or spent > budget_s or n_ent >= (1 << 26):
+            break
+        n_ent *= 4
+    total = plan.n_rows * t_row + plan.ordered_entries * t_dot
+    return {"value": plan.ordered_entries / total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"oracle C port of yk_flat + per-entry dot: {nrow} Y^k rows ({t_row*1e6:.1f} us/row) and "
+                       f"{n_ent} entries ({t_dot*1e9:.0f} ns/entry) on N={n}, extrapolated to "
+                       f"{plan.n_rows} rows + {plan.ordered_entries} entries"),
+            "seconds_measured": round(spent, 2)}
+
+
+def run_reference(args):
+    """--impl reference: the reference algorithm (oracle port) on host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from atomx_b200 import plan as PL
+    from atomx_b200 import workloads as W
+    spec = W.ytterbium_scaleup()
+    ion = W.build_ion(spec)
+    plan = PL.make_plan(ion.kappa, spec.k_max)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(ion, plan, budget_s=6.0)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = float(statistics.median(vals))
+    cb["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": plan.ordered_entries / v * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Dirac-Coulomb spinors)",
+            "config": {"workload": WORKLOAD, "entries_per_step": plan.ordered_entries},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def l2_flush(buf):
+    buf.zero_()
+
+
+def run_gpu(args):
+    import torch
+
+    from atomx_b200 import tables as T
+    from atomx_b200 import workloads as W
+
+    rank, world, local = dist_setup(args.gpus)
+    spec = W.ytterbium_scaleup(seed=2026 + rank)
+    ion = W.build_ion(spec)
+    dev = T.upload_ion(ion)
+    plan = dev.plan
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    engine = args.engine
+    if engine == "split":
+        from atomx_b200.split import SplitEngine
+        eng = SplitEngine(dev)
+        out = None
+
+        def step():
+            return eng.run(stream=stream, upload=False)
+
+        launches_per_step = eng.launches_per_step
+        dom_name = eng.dominant_kernel
+    else:
+        ws = T.Fp64Workspace(dev)
+        out = torch.empty(ws.total, device="cuda", dtype=torch.float64)
+
+        def step():
+            T.run_fp64(dev, ws, out, stream=stream)
+            return out
+
+        launches_per_step = 2
+        dom_name = "fp64tab::contract_kernel"
+
+    # warm-up
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter()
+        for i in range(args.steps):
+            l2_flush(flush)
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        t_wall = time.perf_counter() - t_wall
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    dev_ms_max = allreduce_max(dev_ms, world)
+    entries = float(plan.ordered_entries) * args.steps
+    entries_all = allreduce_sum(entries, world)
+    value = entries_all / (dev_ms_max / 1e3)
+
+    # dominant kernel alone (same stream, same events), for the roofline
+    dom = {}
+    if engine == "fp64":
+        k_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(3)]
+        from atomx_b200 import _native
+        L = _native.load()
+        s = _native.stream_handle(stream)
+        L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                              dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows, dev.r.data_ptr(),
+                              dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(), dev.mi.data_ptr(),
+                              ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, s)
+        for a, b in k_ev:
+            l2_flush(flush)
+            a.record(stream)
+            L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
+                                      ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr(), ws.n_tasks,
+                                      out.data_ptr(), s)
+            b.record(stream)
+        torch.cuda.synchronize()
+        kms = statistics.median(a.elapsed_time(b) for a, b in k_ev)
+        # algorithmic flops per launch: 2*N per computed entry (upper tiles incl. diagonal tiles)
+        computed = sum(min(128, plan.n_of_k(kk) - ti * 128) * min(128, plan.n_of_k(kk) - tj * 128)
+                       for kk in plan.ks for (g, ti, tj) in [(0, a_, b_) for a_ in range((plan.n_of_k(kk) + 127) // 128)
+                                                             for b_ in range(a_, (plan.n_of_k(kk) + 127) // 128)])
+        flops = 2.0 * dev.n * computed
+        peak_tf, src = fp64_peak()
+        dom = {"bound": "tensor", "achieved": flops / (kms / 1e3) / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
+               "frac": flops / (kms / 1e3) / 1e12 / peak_tf, "traffic": None, "kernel": dom_name,
+               "kernel_ms": kms, "peak_source": src, "algorithmic_flops": flops}
+    else:
+        dom = eng.roofline(stream=stream, flush=flush)
+
+    # e2e through the public API with host buffers
+    e2e = e2e_leg(ion, engine, args, world)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if engine == "fp64" else "i8",
+            "data": "synthetic (seeded Dirac-Coulomb spinors, no external dataset)",
+            "config": {"workload": WORKLOAD, "engine": engine, "entries_per_step": plan.ordered_entries,
+                       "unique_entries_per_step": plan.unique_entries, "rows": plan.n_rows,
+                       "l2": "256 MiB flush between timed steps; working set > L2",
+                       "parallelism": f"replicas x{world} (independent ions, no collective)"},
+            "roofline": dom, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(), "wall_s": t_wall}
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(ion, plan)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def fp64_peak():
+    """FP64 tensor peak: cuBLAS DGEMM measured here (not in MEASURED_PEAKS)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float64)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float64)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e) / 1e3
+        best = t if best is None else min(best, t)
+    return 2.0 * n ** 3 / best / 1e12, "measured here: cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 3"
+
+
+def e2e_leg(ion, engine, args, world):
+    """Same metric through the public API from host arrays to a host table."""
+    import torch
+
+    from atomx_b200 import tables as T
+    steps = max(1, min(args.steps, 3))
+    plan = None
+    host_out = None
+    times = []
+    h2d = 0
+    for i in range(steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tab = T.slater_rk_tables(ion, precision=engine)
+        if host_out is None:
+            host_out = torch.empty(tab.values.numel(), dtype=torch.float64, pin_memory=True)
+        host_out.copy_(tab.values, non_blocking=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        plan = tab.plan
+        if i > 0:
+            times.append(dt)
+        h2d = ion.P.nbytes + ion.Q.nbytes
+        del tab
+    tmax = allreduce_max(float(np.median(times)), world)
+    ent = allreduce_sum(float(plan.ordered_entries), world)
+    return {"value": ent / tmax, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(plan.ordered_entries * 8), "steps": steps,
+            "note": "slater_rk_tables(ion) from host coefficients; full table copied to pinned host memory"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--engine", default=os.environ.get("RKB_ENGINE", "fp64"), choices=["split", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,169 @@
+/*
+ * rkb200 — B200-native engine for relativistic radial Slater integrals R^k.
+ *
+ * C-ABI boundary.  Every pointer argument named d_* is a DEVICE pointer on the
+ * calling thread's current CUDA device; `stream` is a cudaStream_t passed as
+ * void* (NULL = legacy default stream).  Arrays are C-order float64 unless a
+ * type says otherwise.  Every entry point is asynchronous with respect to the
+ * host unless stated, returns an rkb_status, and never allocates device memory
+ * except where its comment says so.
+ *
+ * Each entry point names the reference interface (atomx, path relative to
+ * its project root) whose arguments and meaning it mirrors.
+ */
+#ifndef RKB200_H
+#define RKB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RKB_OK = 0,
+    RKB_EINVAL = 1,        /* bad size, stride, multipole or method (reference: ValueError) */
+    RKB_ENONFINITE = 2,    /* non-finite value in a result (reference: FloatingPointError) */
+    RKB_ENOMEM = 3,        /* workspace or admission limit exceeded (reference: MemoryError) */
+    RKB_ETIMEDOUT = 4,     /* a bounded device-side wait gave up */
+    RKB_ECUDA = 5,         /* CUDA runtime error; see rkb_last_error() */
+    RKB_EUNSUPPORTED = 6   /* device is not sm_100 or feature not built */
+} rkb_status;
+
+/* Text of the last error raised on this host thread (never NULL). */
+const char *rkb_last_error(void);
+
+/* Library version string and compiled device architecture. */
+const char *rkb_version(void);
+
+/* 1 if the current device can run the kernels of this library (sm_100), else 0. */
+int rkb_device_supported(void);
+
+/* Largest Gauss order per cell accepted by the Y^k kernels. */
+#define RKB_MAX_NG 32
+
+/* ---------------------------------------------------------------------------
+ * Y^k on the dense Gauss grid.
+ *
+ * rkb_yk_flat mirrors atomx numerics/yk.py:88 yk_flat(rho_flat, r_flat,
+ * w_flat, n, k, nv, ng, mo, mi) -> yk (n,): outward cell sums with the
+ * interpolatory partial matrix mo, inward with mi, Y = r^-(k+1) I_out + r^k I_in.
+ * d_mo, d_mi are ng x ng row-major (atomx yk_partial_matrices).
+ * ------------------------------------------------------------------------- */
+int rkb_yk_flat(const double *d_rho, const double *d_r, const double *d_w, long n, int k,
+                int nv, int ng, const double *d_mo, const double *d_mi, double *d_yk,
+                void *stream);
+
+/* Batched rows: row q reads density d_rho + q*rho_ld, uses multipole
+ * d_row_k[q] and writes d_yk + q*yk_ld.  Same rule as rkb_yk_flat
+ * (atomx numerics/yk.py:157 compute_yk applied per row). */
+int rkb_yk_rows(const double *d_rho, long rho_ld, const int *d_row_k, long nrows,
+                const double *d_r, const double *d_w, int nv, int ng,
+                const double *d_mo, const double *d_mi, double *d_yk, long yk_ld,
+                void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Orbital values on the grid: out[o, iv*ng+m] = sum_s coeff[o, iv+s] * bsp[iv, m, s],
+ * with coefficients at index >= ns taken as zero.
+ * Mirrors atomx numerics/bspline/evaluate.py:71 eval_orbital_on_grid(coeffs,
+ * bsp, nv, ks, ns), batched over n_orb coefficient rows.
+ * ------------------------------------------------------------------------- */
+int rkb_eval_orbitals(const double *d_coeff, long coeff_ld, long n_orb, const double *d_bsp,
+                      int nv, int ng, int ks, int ns, double *d_out, long out_ld, void *stream);
+
+/* Dirac pair densities rho[p] = P[a]P[c] + Q[a]Q[c] for pairs d_pairs[2p], d_pairs[2p+1]
+ * (atomx numerics/bspline/slater_yk.py:193-194). */
+int rkb_pair_density(const double *d_P, const double *d_Q, long orb_ld, const long *d_pairs,
+                     long n_pairs, long n, double *d_rho, long rho_ld, void *stream);
+
+/* Quadrature dots out[e] = sum_i w_i a[ia[e]]_i b[ib[e]]_i (atomx
+ * numerics/bspline/slater.py:130, the slater_rk_poisson contraction). */
+int rkb_weighted_dots(const double *d_a, long a_ld, const double *d_b, long b_ld,
+                      const double *d_w, long n, const long *d_ia, const long *d_ib,
+                      long n_ent, double *d_out, void *stream);
+
+/* O(N^2) direct integrator with the coincident cell split along r = s
+ * (atomx numerics/bspline/slater.py:81 slater_rk_direct).  d_rho13 / d_rho24
+ * are (nv*ng); xi0 is the first node of the ng-point Gauss rule on [-1, 1];
+ * d_outer (order x ng), d_inner (order*order x ng), d_x, d_wx (order) describe
+ * the triangle rule; d_out receives one double. */
+int rkb_slater_direct(const double *d_rho13, const double *d_rho24, const double *d_r,
+                      const double *d_w, int nv, int ng, int k, int order, double xi0,
+                      const double *d_x, const double *d_wx, const double *d_outer,
+                      const double *d_inner, double *d_out, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Plain FP64 table engine (all arithmetic in FP64).
+ *
+ * rkb_table_rows_fp64: for each row q of a plan (pair d_row_pair[q], multipole
+ * d_row_k[q]) form rho from the orbital values, write g_q = w*rho into
+ * d_g + q*ld and Y^k[rho] into d_y + q*ld, padding columns n..ld-1 with 0.
+ *
+ * rkb_table_contract_fp64: for each task t (d_tasks[3t..3t+2] = group, tile_i,
+ * tile_j with tile_j >= tile_i, 128 x 128 tiles) of a group (a multipole)
+ * with rows [d_grp_row0[g], +d_grp_n[g]) computes
+ *     R_g[i][j] = sum_x d_g[row0+i][x] * d_y[row0+j][x]
+ * into the n x n row-major block at d_out + d_grp_out[g]; tiles above the
+ * diagonal are also written transposed, so the block holds every ordered
+ * entry (the table of atomx slater_rk_poisson values over the group's pairs).
+ * ------------------------------------------------------------------------- */
+int rkb_table_rows_fp64(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                        const long *d_row_pair, const int *d_row_k, long nrows,
+                        const double *d_r, const double *d_w, int nv, int ng,
+                        const double *d_mo, const double *d_mi, double *d_g, double *d_y,
+                        long ld, void *stream);
+
+int rkb_table_contract_fp64(const double *d_g, const double *d_y, long ld, long kdim,
+                            const long *d_grp_row0, const long *d_grp_n, const long *d_grp_out,
+                            const int *d_tasks, long n_tasks, double *d_out, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Split-precision engine (factored Green operator + CRT INT8 GEMMs).
+ *
+ * With g = w*rho, atomx's R^k(ac;bd) = g_ac^T G g_bd (numerics/yk.py:88 and
+ * numerics/bspline/slater.py:130).  The engine writes
+ *     R = X_ac.X_bd - Z_ac.Z_bd + left_ac.right_bd
+ * with X, Z from a block Cholesky of the body of G (cells >= 1) including the
+ * rank-one core-body coupling, and left/right the FP64 core (cell 0) Schur
+ * complement terms.
+ *
+ * rkb_split_rows: per plan row q (pair d_row_pair[q], multipole d_row_k[q])
+ * compute [X | Z], scale by 2^(bits - e_q) so |x| < 2^bits, round, and write
+ * int8 residues x mod moduli[i] to d_resA[i][row_base+q][0..kpad) (d_resB, if
+ * not NULL, gets the same with Z negated), 2^(e_q - bits) to d_rowscale, the
+ * core correction vectors (width cwp >= ng) left = g_0, right = S_c g_0 to
+ * d_left / d_right, and to d_cbound[2q], d_cbound[2q+1] the norms |g_0| and
+ * |S_c g_0| divided by 2^e_q (>= the row maximum of |[X | Z]|).  d_ktab holds the
+ * per-k factor tables at offsets d_koff[k] (layout in atomx_b200/split_plan.py).
+ * `moduli` is a HOST array of n_mod pairwise-coprime ints <= 256.
+ *
+ * rkb_split_contract: for every task (group, tile_i, tile_j >= tile_i) the
+ * 128 x 128 tile of R_g is computed as n_mod residue GEMMs of length
+ * d_grp_kdim[g] (multiple of 128) on the tensor cores, CRT-recombined in FP64
+ * with the host constants f_hi/f_lo/M, scaled and corrected, and written (and
+ * mirrored) into the n x n block at d_out + d_grp_out[g], as
+ * rkb_table_contract_fp64 does.  The FP64 core correction of a 32 x 64 block
+ * is skipped when its bound from d_cbound (relative to 2^(e_a + e_b), which
+ * the Schwarz scale of every entry exceeds) is <= corr_floor; pass 0 to
+ * always apply it.  Device waits are bounded; *d_status (device
+ * int, zero on entry) receives RKB_ETIMEDOUT or RKB_ENONFINITE on failure.
+ * ------------------------------------------------------------------------- */
+int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                   const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                   int nv, int ng, const double *d_ktab, const long *d_koff, int bits, int n_mod,
+                   const int *moduli, signed char *d_resA, signed char *d_resB, long kpad,
+                   long row_base, long nrows_total, double *d_rowscale, double *d_left,
+                   double *d_right, double *d_cbound, int cwp, void *stream);
+
+int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, long kpad,
+                       long nrows_total, int n_mod, const int *moduli, const double *f_hi,
+                       const double *f_lo, double M, const double *d_rowscale,
+                       const double *d_left, const double *d_right, const double *d_cbound,
+                       double corr_floor, int cw, int cwp,
+                       const long *d_grp_row0, const long *d_grp_n, const long *d_grp_kdim,
+                       const long *d_grp_out, const int *d_tasks, long n_tasks, double *d_out,
+                       int *d_status, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RKB200_H */

@@ -17,7 +17,10 @@ atomx.  What each file holds:
                          ``slater_rk_poisson``, a few ``compute_slater_rk``
                          and ``slater_rk_direct`` values.
 * ytterbium_scaleup.npz  Z=70, 200 rotated spinors: coefficient digest,
-                         sampled Y^k rows and sampled R^k entries.
+                         sampled Y^k rows with their densities, sampled R^k
+                         entries.  (Spinors from LAPACK eigensolvers differ in
+                         the last bits between hosts, so device tests use the
+                         stored densities, not regenerated ones.)
 * xenon_ci_table.npz     Z=54, 300 spinors, N=2112: digest, sampled entries.
 * batch_ions.npz         three ions of the uneven batch: digests, samples.
 * hydrogenic.npz         atomx physics grid (ks=9, Z=1, r_max=50): nodes and
@@ -108,11 +111,11 @@ def main():
         Qg = np.array([eval_Q(c, bd).ravel() for c in ion.Q])
         rng = np.random.default_rng(seed)
         rsel = np.sort(rng.choice(plan.n_rows, size=min(n_rows, plan.n_rows), replace=False))
-        yrows = []
+        yrows, rrho = [], []
         for q in rsel:
             a, c = plan.pairs[plan.row_pair[q]]
-            yrows.append(compute_yk((Pg[a] * Pg[c] + Qg[a] * Qg[c]).reshape(nv, ng), gr, grw, nv, ng,
-                                    int(plan.row_k[q])).ravel())
+            rrho.append(Pg[a] * Pg[c] + Qg[a] * Qg[c])
+            yrows.append(compute_yk(rrho[-1].reshape(nv, ng), gr, grw, nv, ng, int(plan.row_k[q])).ravel())
         ents = []
         for _ in range(n_ent):
             k = int(rng.choice(plan.ks))
@@ -124,7 +127,7 @@ def main():
             r24 = Pg[b] * Pg[d] + Qg[b] * Qg[d]
             ents.append((k, i, j, slater_rk_poisson(r13, r24, gr, grw, nv, ng, k)))
         return dict(digest=np.array(ion.coefficient_digest()), row_index=rsel, yk_rows=np.array(yrows),
-                    entries=np.array(ents))
+                    row_rho=np.array(rrho), row_k=plan.row_k[rsel], entries=np.array(ents))
 
     c2 = sampled(W.ytterbium_scaleup(), "ytterbium_scaleup.npz")
     np.savez_compressed(os.path.join(HERE, "ytterbium_scaleup.npz"), **c2)

@@ -1,0 +1,98 @@
+"""CPU emulation of the split engine's two kernels (test helper).
+
+``emulate_rows`` follows split_rows_kernel step by step on the packed factor
+tables (same layout, same per-row power-of-two scaling, same residue rule);
+``emulate_contract`` follows crt_syrk_kernel: exact int64 residue products
+per modulus, the same reduction to [-128, 127], the same CRT constants and
+FP64 recombination.  Tests compare the device buffers and tables with these.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from atomx_b200.split_plan import factor_table_layout
+
+
+def unpack_table(flat, off, nv, ng):
+    o = factor_table_layout(nv, ng)
+    n = nv * ng
+    t = flat[off:]
+    nz = int(t[o["nz"]])
+    z = t[o["z"]:o["z"] + nz * (ng + 1)].reshape(nz, ng + 1) if nz else np.zeros((0, ng + 1))
+    return dict(u=t[:n].reshape(nv, ng), ell=t[o["ell"]:o["ell"] + n].reshape(nv, ng),
+                Lb=t[o["Lb"]:o["Lb"] + nv * ng * ng].reshape(nv, ng, ng),
+                C=t[o["C"]:o["C"] + nv * ng].reshape(nv, ng), v0=t[o["v0"]:o["v0"] + ng],
+                Sc=t[o["Sc"]:o["Sc"] + ng * ng].reshape(ng, ng), zcell=z[:, 0].astype(int), zvec=z[:, 1:])
+
+
+def transform_rows(g, F, nv, ng):
+    """[X | Z], left, right for rows g (rows, N) with one factor table F."""
+    rows = g.shape[0]
+    gb = g.reshape(rows, nv, ng)
+    d = np.einsum("qmi,mi->qm", gb, F["u"])
+    d[:, 0] = 0.0
+    suf = np.cumsum(d[:, ::-1], axis=1)[:, ::-1]
+    tn = np.concatenate([suf[:, 1:], np.zeros((rows, 1))], axis=1)
+    g0 = gb[:, 0, :]
+    alpha = g0 @ F["v0"]
+    X = np.einsum("mij,qmi->qmj", F["Lb"], gb) + F["C"][None] * tn[:, :, None] + F["ell"][None] * alpha[:, None, None]
+    X = X[:, 1:, :].reshape(rows, -1)
+    Z = np.stack([gb[:, m, :] @ z for m, z in zip(F["zcell"], F["zvec"])], axis=1) if len(F["zcell"]) else \
+        np.zeros((rows, 0))
+    left = g0
+    right = g0 @ F["Sc"].T
+    return X, Z, left, right
+
+
+def residues(xq, moduli):
+    out = []
+    for m in moduli:
+        r = xq - m * np.rint(xq / m)
+        r = np.where(r > 127, r - m, r)
+        r = np.where(r < -128, r + m, r)
+        out.append(r.astype(np.int64))
+    return out
+
+
+def crt_value(res_list, moduli, f_hi, f_lo, M):
+    yh = np.zeros(res_list[0].shape)
+    yl = np.zeros(res_list[0].shape)
+    for r, fh, fl in zip(res_list, f_hi, f_lo):
+        yh = yh + r * fh
+        yl = yl + r * fl
+    return (yh - np.rint(yh)) * M + yl * M
+
+
+def crt_exact(res_list, moduli):
+    """Exact symmetric CRT with Python integers (|x| < M/2)."""
+    ms = [int(m) for m in moduli]
+    M = 1
+    for m in ms:
+        M *= m
+    W = [(M // m) * pow((M // m) % m, -1, m) for m in ms]
+    shape = res_list[0].shape
+    flat = [np.asarray(r).ravel().tolist() for r in res_list]
+    out = np.empty(len(flat[0]), dtype=np.float64)
+    for idx in range(len(flat[0])):
+        x = sum(int(flat[i][idx]) * W[i] for i in range(len(ms))) % M
+        if x > M // 2:
+            x -= M
+        out[idx] = float(x)
+    return out.reshape(shape)
+
+
+def reduce_mod(v, m):
+    r = v - m * np.rint(v / m).astype(np.int64)
+    for _ in range(2):
+        r = np.where(r < -128, r + m, r)
+        r = np.where(r > 127, r - m, r)
+    return r
+
+
+def emulate_table(Ares, Bres, rowscale, left, right, moduli, f_hi, f_lo, M):
+    """One symmetric table from residue rows (lists per modulus of (n, K))."""
+    res = []
+    for a, b, m in zip(Ares, Bres, moduli):
+        res.append(reduce_mod(a.astype(np.int64) @ b.astype(np.int64).T, int(m)))
+    x = crt_value(res, moduli, f_hi, f_lo, M)
+    return x * np.outer(rowscale, rowscale) + left @ right.T

@@ -1,0 +1,90 @@
+"""CPU checks of the split engine's planning: the packed factor tables, the
+factored identity R = X.X - Z.Z + left.right against the oracle, the CRT
+constants, and the fixed-point error model."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from split_emulation import crt_value, residues, transform_rows, unpack_table
+
+
+def _ion_rows(name, n_pairs=120, seed=0):
+    from atomx_b200 import plan as PL
+    from atomx_b200 import workloads as W
+    spec = getattr(W, name)()
+    ion = W.build_ion(spec)
+    bd = ion.bsp
+    Pg = np.array([oracle.eval_P(c, bd).ravel() for c in ion.P])
+    Qg = np.array([oracle.eval_Q(c, bd).ravel() for c in ion.Q])
+    plan = PL.make_plan(ion.kappa, spec.k_max)
+    return spec, ion, bd, Pg, Qg, plan
+
+
+@pytest.mark.parametrize("name,ks", [("neon_small", [0, 1, 2]), ("ytterbium_scaleup", [0, 5, 12])])
+def test_factored_identity_matches_oracle(name, ks):
+    from atomx_b200.split import factors_for_grid
+    from atomx_b200.split_plan import pack_factors
+    spec, ion, bd, Pg, Qg, plan = _ion_rows(name)
+    gr, grw = bd["gr"], bd["grw"]
+    nv, ng = gr.shape
+    facs = factors_for_grid(gr.ravel(), ng, ks)
+    flat, offs = pack_factors([facs[k] for k in ks])
+    rng = np.random.default_rng(1)
+    for i, k in enumerate(ks):
+        F = unpack_table(flat, offs[i], nv, ng)
+        pk = plan.pairs_of_k[k]
+        sel = pk[rng.choice(pk.shape[0], size=min(60, pk.shape[0]), replace=False)]
+        rho = np.array([Pg[a] * Pg[c] + Qg[a] * Qg[c] for a, c in plan.pairs[sel]])
+        g = rho * grw.reshape(1, -1)
+        y = oracle.yk_rows(rho, k, gr, grw, nv, ng)
+        ref = g @ y.T
+        X, Z, left, right = transform_rows(g, F, nv, ng)
+        got = X @ X.T - Z @ Z.T + left @ right.T
+        d = np.abs(np.diag(ref))
+        err = np.abs(got - ref) / np.sqrt(np.outer(d, d))
+        assert err.max() < 1e-13, (name, k, err.max())
+
+
+def test_crt_constants_reconstruct_integers():
+    from atomx_b200.split_plan import crt_constants, moduli_needed
+    for bits, kdim in ((36, 896), (36, 2176), (40, 1024)):
+        nm = moduli_needed(bits, kdim)
+        ms, fh, fl, M = crt_constants(nm)
+        assert M > 2 * kdim * 2.0 ** (2 * bits)
+        rng = np.random.default_rng(bits)
+        bound = kdim * 2 ** (2 * bits)
+        xs = [int(v) for v in rng.integers(-2**62, 2**62, size=200)] + [bound, -bound, 0, 1, -1]
+        xs = [x % (2 * bound) - bound for x in xs]
+        for x in xs:
+            res = [np.array([((x + int(m) // 2) % int(m)) - int(m) // 2]) for m in ms]  # any representative
+            got = float(crt_value(res, ms, fh, fl, M)[0])
+            assert abs(got - float(x)) <= 2.0 ** -50 * abs(float(x)) + 8.0, (bits, x, got)
+        # f_hi exactness: multiples of 2^-42
+        assert np.all(fh * 2.0 ** 42 == np.rint(fh * 2.0 ** 42))
+
+
+def test_fixed_point_split_error_model():
+    """36-bit rows: Schwarz-relative error ~ 2^-36 on the Z=70 ion."""
+    from atomx_b200.split import factors_for_grid
+    spec, ion, bd, Pg, Qg, plan = _ion_rows("ytterbium_scaleup")
+    gr, grw = bd["gr"], bd["grw"]
+    nv, ng = gr.shape
+    for k in (0, 12):
+        F = factors_for_grid(gr.ravel(), ng, [k])[k]
+        F = dict(F, zcell=F["zcell"], zvec=F["zvec"])
+        pk = plan.pairs_of_k[k]
+        sel = pk[np.random.default_rng(k).choice(pk.shape[0], size=min(200, pk.shape[0]), replace=False)]
+        rho = np.array([Pg[a] * Pg[c] + Qg[a] * Qg[c] for a, c in plan.pairs[sel]])
+        g = rho * grw.reshape(1, -1)
+        X, Z, left, right = transform_rows(g, F, nv, ng)
+        XZ = np.concatenate([X, Z], axis=1)
+        e = np.frexp(np.abs(XZ).max(axis=1))[1]
+        s = np.ldexp(1.0, 36 - e)[:, None]
+        q = np.rint(XZ * s) / s
+        qm = q.copy()
+        qm[:, X.shape[1]:] *= -1
+        got = q @ qm.T + left @ right.T
+        ref = XZ @ np.concatenate([X, -Z], axis=1).T + left @ right.T
+        d = np.abs(np.diag(ref))
+        err = np.abs(got - ref) / np.sqrt(np.outer(d, d))
+        assert err.max() < 5e-11, (k, err.max())
