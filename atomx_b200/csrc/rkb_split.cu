@@ -8,9 +8,10 @@
 //      the exclusive suffix sums T_m = sum_{m'>m} d_m' (warp-shuffle scans);
 //      X_m = L_mm^T g_m + c_m T_m + ell_m (v_0.g_0);  Z_e = z_e . g_{cell(e)};
 //      FP64 core terms left = g_0, right = S_c g_0 (core Schur complement).
-//      Each row [X | Z] is scaled by a power of two to |x| < 2^bits, rounded
-//      to an integer x~ and written as int8 residues x~ mod m_i (and the B copy
-//      with Z negated) in a [modulus][row][kpad] layout.
+//      The FP64 row [X | Z] goes to a scratch buffer with its power-of-two
+//      scale (|x| < 2^bits); split_residues_kernel then rounds it to integers
+//      x~ and writes int8 residues x~ mod m_i (and the B copy with Z negated)
+//      in a [modulus][row][kpad] layout, one 16-byte store per modulus.
 //
 // K3s  crt_syrk_kernel  (persistent, one CTA per SM, 10 warps)
 //      warp 0: TMA producer — 128x128-byte boxes (SWIZZLE_128B) of the A and B
@@ -18,11 +19,13 @@
 //      warp 1: TMEM owner + MMA issuer — tcgen05.mma.kind::i8, M=N=128, K=32,
 //              int32 accumulators in a double-buffered TMEM tile;
 //      warps 2-9: epilogue (4 TMEM lane quarters x 2 column halves) — per
-//              modulus: TMEM -> registers, reduce mod m_i, pack 4 residues per
-//              32-bit word (groups of 4 moduli parked in TMEM columns 256..511,
-//              the last group kept in registers); per tile: CRT in FP64 (exact
-//              split constants), scale, add the core correction, store the
-//              tile and its transpose.
+//              modulus: TMEM -> registers, reduce to [0, m) with integer
+//              operations, merge each even/odd pair of moduli into a 16-bit
+//              digit mod m_e m_o (two digits per 32-bit word; words of four
+//              moduli parked in TMEM columns 256..511, the last word kept in
+//              registers); per tile: CRT over the digits in FP64 (exact split
+//              constants), scale, add the core correction when it is not
+//              screened out, store the tile and its transpose.
 //      Every mbarrier wait is bounded; on timeout the kernel records
 //      RKB_ETIMEDOUT in *status and every role drains and returns.
 #include <cuda.h>
@@ -49,10 +52,11 @@ struct RowsArgs {
     const long *koff;  // by k
     int bits, n_mod;
     int mod[MAXMOD];
-    double inv_mod[MAXMOD];
+    uint32_t magic[MAXMOD], c20[MAXMOD], bias[MAXMOD];  // 2^32/m + 1, 2^20 mod m, m * 2^20
     signed char *resA, *resB;  // [n_mod][nrows_total][kpad]; resB may be null
     long kpad, row_base, nrows_total;
     double *rowscale, *left, *right, *cbound;
+    double *xwork;  // scratch rows [X | Z | 0] (row stride kpad)
     int cwp;
 };
 
@@ -63,25 +67,43 @@ __device__ __forceinline__ double rho_at(const RowsArgs &a, long q, long i) {
                      __dmul_rn(a.Q[x * a.orb_ld + i], a.Q[c * a.orb_ld + i]));
 }
 
-// x in (-2^bits, 2^bits) integer-valued double -> residue in [-128, 127]
-__device__ __forceinline__ int residue_of(double x, int m, double inv_m) {
-    double q = rint(x * inv_m);
-    int r = (int)fma(-q, (double)m, x);
-    if (r > 127) r -= m;
-    if (r < -128) r += m;
-    return r;
+// x mod m in [0, m) for 0 <= x < 2^32 with integer operations only:
+// q = hi32(x * (floor(2^32/m) + 1)) exceeds x/m by less than x/2^32 < 1, so it
+// is floor(x/m) or one more, and one conditional add repairs the remainder.
+__device__ __forceinline__ uint32_t umod_small(uint32_t x, uint32_t m, uint32_t magic) {
+    const uint32_t q = __umulhi(x, magic);
+    int r = (int)(x - q * m);
+    return (uint32_t)(r + (r < 0 ? (int)m : 0));
 }
 
+// Centred int8 residue (as a byte) of an integer x = hi * 2^20 + lo, |hi| <= 2^20, 0 <= lo < 2^20.
+__device__ __forceinline__ uint32_t residue_i8(int hi, uint32_t lo, uint32_t m, uint32_t magic, uint32_t c20,
+                                               uint32_t bias) {
+    // (hi mod m) * (2^20 mod m) + (lo mod m): every operand nonnegative and < 2^29
+    const uint32_t h = umod_small((uint32_t)(hi + (int)bias), m, magic);
+    const uint32_t l = umod_small(lo, m, magic);
+    const uint32_t r = umod_small(h * c20 + l, m, magic);
+    const int rc = (int)r - (r > 127u ? (int)m : 0);
+    return (uint32_t)rc & 0xffu;
+}
+
+// One warp per row.  Shared memory per warp: g (n doubles) and the per-cell
+// suffix sums (nv doubles).  Cells are processed by lane groups of ng lanes
+// (lane = node of a cell), so shared and global accesses are consecutive
+// across lanes.  The FP64 row [X | Z | 0...] goes to the caller's scratch
+// buffer; split_residues_kernel turns it into int8 residues.
 template <int NG>
 __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
-    constexpr int NGMAX = NG > 0 ? NG : RKB_MAX_NG;
     const int ng = NG > 0 ? NG : a.ng;
     const int nv = a.nv;
     const long n = (long)nv * ng;
     extern __shared__ double sm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *g = sm + (long)wib * (n + nv);
-    double *tsuf = g + n;  // exclusive suffix sums per cell
+    // segment lengths rounded to even counts of doubles keep every segment 16-byte aligned
+    const long np = (n + 1) & ~1L, nvp = (nv + 1) & ~1L;
+    const long per_warp = np + nvp;
+    double *g = sm + (long)wib * per_warp;
+    double *tsuf = g + np;
     const long q = (long)blockIdx.x * (blockDim.x >> 5) + wib;
     if (q >= a.nrows) return;
     const int k = a.row_k[q];
@@ -95,6 +117,10 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
     const int nz = (int)Sc[ng * ng];
     const double *zt = Sc + ng * ng + 1;
     const long kbody = (long)(nv - 1) * ng;
+    // lane groups: cpp cells per pass, lane -> (cell offset, node)
+    const int cpp = 32 / ng;
+    const int sub = lane / ng, node = lane - sub * ng;
+    const bool glane = sub < cpp;
 
     for (long i = lane; i < n; i += 32) g[i] = __dmul_rn(a.w[i], rho_at(a, q, i));
     __syncwarp();
@@ -103,35 +129,46 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
     for (int j = lane; j < ng; j += 32) alpha = fma(v0[j], g[j], alpha);
     alpha = warp_sum(alpha);
 
-    // suffix sums over body cells (cell 0 contributes nothing)
+    // cell dots d_m = u_m . g_m (m >= 1) by lane groups, segmented shuffle sums
+    for (int m0 = 0; m0 < nv; m0 += cpp) {
+        const int m = m0 + sub;
+        double p = 0.0;
+        if (glane && m >= 1 && m < nv) p = u[(long)m * ng + node] * g[(long)m * ng + node];
+        // sum over the ng lanes of the group (groups never straddle: lanes >= cpp*ng idle)
+        double tot = 0.0;
+        for (int t = 0; t < ng; ++t) tot += __shfl_sync(0xffffffffu, p, sub * ng + t < 32 ? sub * ng + t : lane);
+        if (glane && node == 0 && m < nv) tsuf[m] = (m >= 1) ? tot : 0.0;
+    }
+    __syncwarp();
+    // exclusive suffix sums over cells: lane l owns cell (end - l) of each chunk
     const int nch = (nv + 31) >> 5;
     double carry = 0.0;
     for (int c = 0; c < nch; ++c) {
-        int m = nv - 1 - ((c << 5) + lane);
-        double d = 0.0;
-        if (m >= 1) {
-            for (int j = 0; j < ng; ++j) d = fma(u[(long)m * ng + j], g[(long)m * ng + j], d);
-        }
-        double incl = warp_inclusive_scan(d, lane);
-        double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        const int m = nv - 1 - ((c << 5) + lane);
+        const double d = m >= 0 ? tsuf[m] : 0.0;
+        const double incl = warp_inclusive_scan(d, lane);
+        const double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        __syncwarp();
         if (m >= 0) tsuf[m] = lane == 0 ? carry : carry + excl;
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     __syncwarp();
 
-    // pass A: row maximum of |[X | Z]|
+    // the row [X | Z | 0...] into the scratch row, with its maximum
+    const long grow = a.row_base + q;  // row index in the residue matrices
+    double *xs = a.xwork + grow * a.kpad;
     double amax = 0.0;
-    for (int m = 1 + lane; m < nv; m += 32) {
-        const double *L = Lb + (long)m * ng * ng;
-        const double *gm = g + (long)m * ng;
-        double t = tsuf[m];
-#pragma unroll
-        for (int j = 0; j < NGMAX; ++j) {
-            if (j < ng) {
-                double x = fma(ell[(long)m * ng + j], alpha, C[(long)m * ng + j] * t);
-                for (int i = j; i < ng; ++i) x = fma(L[i * ng + j], gm[i], x);
-                amax = fmax(amax, fabs(x));
-            }
+    bool bad = false;  // fmax drops NaNs, so non-finite values are tracked apart
+    for (int m0 = 1; m0 < nv; m0 += cpp) {
+        const int m = m0 + sub;
+        if (glane && m < nv) {
+            const double *L = Lb + (long)m * ng * ng;
+            const double *gm = g + (long)m * ng;
+            double x = fma(ell[(long)m * ng + node], alpha, C[(long)m * ng + node] * tsuf[m]);
+            for (int i = node; i < ng; ++i) x = fma(L[i * ng + node], gm[i], x);
+            xs[(long)(m - 1) * ng + node] = x;
+            amax = fmax(amax, fabs(x));
+            bad |= !isfinite(x);
         }
     }
     for (int e = lane; e < nz; e += 32) {
@@ -139,92 +176,105 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
         const double *gm = g + (long)ze[0] * ng;
         double x = 0.0;
         for (int i = 0; i < ng; ++i) x = fma(ze[1 + i], gm[i], x);
+        xs[kbody + e] = x;
         amax = fmax(amax, fabs(x));
+        bad |= !isfinite(x);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
 
+    for (long c = kbody + nz + lane; c < a.kpad; c += 32) xs[c] = 0.0;
     int ex = 0;
-    double scale = 0.0, inv_scale = 0.0;
+    double inv_scale = 0.0;
     if (amax > 0.0 && isfinite(amax)) {
         frexp(amax, &ex);  // amax < 2^ex
-        scale = ldexp(1.0, a.bits - ex);
         inv_scale = ldexp(1.0, ex - a.bits);
     }
-    const long grow = a.row_base + q;  // row index in the residue matrices
 
-    // pass B: quantise and write residues (lane = cell -> ng contiguous bytes)
-    for (int m = 1 + lane; m < nv; m += 32) {
-        const double *L = Lb + (long)m * ng * ng;
-        const double *gm = g + (long)m * ng;
-        double t = tsuf[m];
-        double xq[NGMAX];
-#pragma unroll
-        for (int j = 0; j < NGMAX; ++j) {
-            if (j < ng) {
-                double x = fma(ell[(long)m * ng + j], alpha, C[(long)m * ng + j] * t);
-                for (int i = j; i < ng; ++i) x = fma(L[i * ng + j], gm[i], x);
-                xq[j] = rint(x * scale);
-            }
-        }
-        const long col = (long)(m - 1) * ng;
-        for (int md = 0; md < a.n_mod; ++md) {
-            signed char *dA = a.resA + ((long)md * a.nrows_total + grow) * a.kpad + col;
-            signed char *dB = a.resB ? a.resB + ((long)md * a.nrows_total + grow) * a.kpad + col : nullptr;
-#pragma unroll
-            for (int j = 0; j < NGMAX; ++j) {
-                if (j < ng) {
-                    signed char r = (signed char)residue_of(xq[j], a.mod[md], a.inv_mod[md]);
-                    dA[j] = r;
-                    if (dB) dB[j] = r;
-                }
-            }
-        }
-    }
-    for (int e = lane; e < nz; e += 32) {
-        const double *ze = zt + (long)e * (ng + 1);
-        const double *gm = g + (long)ze[0] * ng;
-        double x = 0.0;
-        for (int i = 0; i < ng; ++i) x = fma(ze[1 + i], gm[i], x);
-        double xq = rint(x * scale);
-        for (int md = 0; md < a.n_mod; ++md) {
-            long o = ((long)md * a.nrows_total + grow) * a.kpad + kbody + e;
-            int r = residue_of(xq, a.mod[md], a.inv_mod[md]);
-            a.resA[o] = (signed char)r;
-            if (a.resB) a.resB[o] = (signed char)residue_of(-xq, a.mod[md], a.inv_mod[md]);
-        }
-    }
-    // zero padding columns
-    for (long c = kbody + nz + lane; c < a.kpad; c += 32) {
-        for (int md = 0; md < a.n_mod; ++md) {
-            long o = ((long)md * a.nrows_total + grow) * a.kpad + c;
-            a.resA[o] = 0;
-            if (a.resB) a.resB[o] = 0;
-        }
-    }
     // FP64 core correction: left = g_0, right = S_c g_0, and the screen bounds
     double *lf = a.left + grow * a.cwp, *rt = a.right + grow * a.cwp;
     double n1 = 0.0, n2 = 0.0;
     for (int i = lane; i < a.cwp; i += 32) {
-        double gi = 0.0, s = 0.0;
+        double gi = 0.0, sacc = 0.0;
         if (i < ng) {
             gi = g[i];
-            for (int j = 0; j < ng; ++j) s = fma(Sc[i * ng + j], g[j], s);
+            for (int j = 0; j < ng; ++j) sacc = fma(Sc[i * ng + j], g[j], sacc);
         }
         lf[i] = gi;
-        rt[i] = s;
+        rt[i] = sacc;
         n1 = fma(gi, gi, n1);
-        n2 = fma(s, s, n2);
+        n2 = fma(sacc, sacc, n2);
     }
     n1 = warp_sum(n1);
     n2 = warp_sum(n2);
+    bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
-        a.rowscale[grow] = inv_scale;
+        // a non-finite row gets a NaN scale: its residues are zero and every
+        // entry it reaches is NaN, which the contraction reports
+        a.rowscale[grow] = bad ? __longlong_as_double(0x7ff8000000000000LL) : inv_scale;
         // bounds of |g_0| and |S_c g_0| relative to 2^ex (>= the row maximum of
         // |[X | Z]|); a zero row keeps them infinite (never screened)
         const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
         a.cbound[grow * 2] = sqrt(n1) * rel;
         a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+    }
+}
+
+
+// Residues of the scaled rows: one thread per (row, 16 columns).  x = rint(X *
+// 2^(bits - e_row)) is an exact integer with |x| <= 2^bits; each modulus gets
+// one 16-byte store (and the B copy negates the row's Z columns).
+__global__ void __launch_bounds__(256) split_residues_kernel(RowsArgs a, const int *__restrict__ z_count) {
+    const long per_row = a.kpad / 16;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.nrows * per_row) return;
+    const long q = t / per_row, c0 = (t - q * per_row) * 16;
+    const long grow = a.row_base + q;
+    const double rs = a.rowscale[grow];
+    const double scale = rs > 0.0 ? 1.0 / rs : 0.0;  // an exact power of two
+    const double *xs = a.xwork + grow * a.kpad + c0;
+    int hi[16];
+    uint32_t lo[16];
+#pragma unroll
+    for (int j = 0; j < 16; j += 2) {
+        const double2 v = *reinterpret_cast<const double2 *>(xs + j);
+        double y0 = v.x * scale, y1 = v.y * scale;
+        y0 = fabs(y0) <= 0x1p40 ? y0 : 0.0;  // NaN rows (and a zero scale) give zeros
+        y1 = fabs(y1) <= 0x1p40 ? y1 : 0.0;
+        const long long x0 = (long long)rint(y0), x1 = (long long)rint(y1);
+        hi[j] = (int)(x0 >> 20);
+        lo[j] = (uint32_t)(x0 & 0xfffffLL);
+        hi[j + 1] = (int)(x1 >> 20);
+        lo[j + 1] = (uint32_t)(x1 & 0xfffffLL);
+    }
+    const long kbody = (long)(a.nv - 1) * a.ng;
+    const long zhi = kbody + z_count[a.row_k[q]];
+    const bool anyz = a.resB != nullptr && c0 + 16 > kbody && c0 < zhi;
+    for (int md = 0; md < a.n_mod; ++md) {
+        const uint32_t m = (uint32_t)a.mod[md], magic = a.magic[md], c20 = a.c20[md], bias = a.bias[md];
+        uint32_t w[4], wb[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            uint32_t va = 0u, vb = 0u;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const int j = 4 * i + s;
+                const uint32_t r = residue_i8(hi[j], lo[j], m, magic, c20, bias);
+                va |= r << (8 * s);
+                uint32_t rb = r;
+                if (anyz && c0 + j >= kbody && c0 + j < zhi) {
+                    int nr = -(int)(int8_t)(uint8_t)r;  // residue of -x, centred again
+                    nr -= nr > 127 ? (int)m : 0;
+                    rb = (uint32_t)nr & 0xffu;
+                }
+                vb |= rb << (8 * s);
+            }
+            w[i] = va;
+            wb[i] = vb;
+        }
+        const long o = ((long)md * a.nrows_total + grow) * a.kpad + c0;
+        *reinterpret_cast<uint4 *>(a.resA + o) = make_uint4(w[0], w[1], w[2], w[3]);
+        if (a.resB) *reinterpret_cast<uint4 *>(a.resB + o) = make_uint4(wb[0], wb[1], wb[2], wb[3]);
     }
 }
 
@@ -255,8 +305,10 @@ struct CrtArgs {
     int *status;
     int n_mod;
     int mod[MAXMOD];
-    float inv_mod[MAXMOD];
-    double f_hi[MAXMOD], f_lo[MAXMOD];
+    uint32_t magic[MAXMOD];   // floor(2^32 / m) + 1
+    uint32_t bias[MAXMOD];    // m * 2^18: makes every accumulator nonnegative
+    uint32_t pinv[MAXMOD / 2];  // m_2p^-1 mod m_2p+1
+    double f_hi[MAXMOD], f_lo[MAXMOD];  // per merged digit
     double M;
 };
 
@@ -353,23 +405,13 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t *v) {
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// int32 accumulator -> a representative of v mod m in [-128, 127].  The
-// float quotient is off by at most one for |v| < 2^25, which one conditional
-// add and one conditional subtract absorb.
-__device__ __forceinline__ uint32_t residue_byte(int v, int m, float inv_m) {
-    int q = __float2int_rn(__int2float_rn(v) * inv_m);
-    int r = v - q * m;
-    r += (r < -128) ? m : 0;
-    r -= (r > 127) ? m : 0;
-    return (uint32_t)r & 0xffu;
-}
-
 template <int NMOD>
 __global__ void __launch_bounds__(THREADS, 1)
     crt_syrk_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                     const __grid_constant__ CrtArgs p) {
     constexpr int PARKED = (NMOD - 1) >> 2;  // groups of four moduli parked in TMEM (0..2)
     constexpr int LASTG = PARKED;            // group kept in registers
+    constexpr int NDIG = (NMOD + 1) / 2;     // merged CRT digits
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char *ring = base;
@@ -479,15 +521,35 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint32_t aph = (acc_it >> 1) & 1u;
                 if (!mbar_wait(&accf[buf], aph, status)) { ok = false; break; }
                 tc_fence_after();
-                const int m = p.mod[md];
-                const float im = p.inv_mod[md];
+                const uint32_t m = (uint32_t)p.mod[md], magic = p.magic[md], bias = p.bias[md];
+                const int fsh = 16 * ((md >> 1) & 1);  // 16-bit field of this pair in the word
+                if ((md & 1) == 0) {
+                    // even modulus: park r_e in its pair field
 #pragma unroll
-                for (int c = 0; c < EPI_COLS / 16; ++c) {
-                    uint32_t v[16];
-                    tmem_ld16(tmem + lane_off + (uint32_t)(buf * BN) + col0 + (uint32_t)(c * 16), v);
-                    tmem_wait_ld();
+                    for (int c = 0; c < EPI_COLS / 16; ++c) {
+                        uint32_t v[16];
+                        tmem_ld16(tmem + lane_off + (uint32_t)(buf * BN) + col0 + (uint32_t)(c * 16), v);
+                        tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) pk[c * 16 + j] |= residue_byte((int)v[j], m, im) << (8 * (md & 3));
+                        for (int j = 0; j < 16; ++j) pk[c * 16 + j] |= umod_small(v[j] + bias, m, magic) << fsh;
+                    }
+                } else {
+                    // odd modulus: merge with the parked r_e into a digit mod m_e m_o
+                    const uint32_t me = (uint32_t)p.mod[md - 1], inv = p.pinv[md >> 1];
+#pragma unroll
+                    for (int c = 0; c < EPI_COLS / 16; ++c) {
+                        uint32_t v[16];
+                        tmem_ld16(tmem + lane_off + (uint32_t)(buf * BN) + col0 + (uint32_t)(c * 16), v);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const uint32_t ro = umod_small(v[j] + bias, m, magic);
+                            const uint32_t word = pk[c * 16 + j];
+                            const uint32_t re = (word >> fsh) & 0xffffu;
+                            const uint32_t t = umod_small((ro + 2u * m - re) * inv, m, magic);
+                            pk[c * 16 + j] = (word & ~(0xffffu << fsh)) | ((re + me * t) << fsh);
+                        }
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -538,12 +600,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int j = 0; j < FC; ++j) {
                     double yh = 0.0, yl = 0.0;
 #pragma unroll
-                    for (int md = 0; md < NMOD; ++md) {
+                    for (int dg = 0; dg < NDIG; ++dg) {
+                        const int md = 2 * dg;              // first modulus of the digit
                         const int grp = md >> 2;
                         const uint32_t word = grp == LASTG ? pk[c * FC + j] : (grp == 0 ? w0[j] : w1[j]);
-                        const double r = (double)(int)(signed char)(word >> (8 * (md & 3)));
-                        yh = fma(r, p.f_hi[md], yh);
-                        yl = fma(r, p.f_lo[md], yl);
+                        const uint32_t dv = (word >> (16 * ((md >> 1) & 1))) & 0xffffu;
+                        // exact int -> double: (2^52 + dv) - 2^52
+                        const double r = __hiloint2double(0x43300000, (int)dv) - 4503599627370496.0;
+                        yh = fma(r, p.f_hi[dg], yh);
+                        yl = fma(r, p.f_lo[dg], yl);
                     }
                     const long b = b0 + c * FC + j;
                     const double rs_b = b < n ? __ldg(p.rowscale + row0 + b) : 0.0;
@@ -643,7 +708,8 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
                               int ng, const double *d_ktab, const long *d_koff, int bits, int n_mod,
                               const int *moduli, signed char *d_resA, signed char *d_resB, long kpad,
                               long row_base, long nrows_total, double *d_rowscale, double *d_left,
-                              double *d_right, double *d_cbound, int cwp, void *stream) {
+                              double *d_right, double *d_cbound, int cwp, double *d_xwork,
+                              const int *d_zcount, void *stream) {
     RKB_CHECK_ARG(nv >= 2 && ng >= 1 && ng <= RKB_MAX_NG, "invalid grid (nv=%d, ng=%d)", nv, ng);
     RKB_CHECK_ARG(bits >= 8 && bits <= 50, "bits must be in [8, 50] (got %d)", bits);
     RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
@@ -658,16 +724,28 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
     a.nrows = nrows; a.w = d_w; a.nv = nv; a.ng = ng; a.ktab = d_ktab; a.koff = d_koff; a.bits = bits;
     a.n_mod = n_mod;
     for (int i = 0; i < MAXMOD; ++i) {
-        a.mod[i] = i < n_mod ? moduli[i] : 1;
-        a.inv_mod[i] = 1.0 / (double)a.mod[i];
+        const int m = i < n_mod ? moduli[i] : 256;
+        RKB_CHECK_ARG(m >= 2 && m <= 256, "moduli must lie in [2, 256]");
+        a.mod[i] = m;
+        a.magic[i] = (uint32_t)((1ULL << 32) / (unsigned long long)m + 1ULL);
+        a.c20[i] = (uint32_t)((1u << 20) % (uint32_t)m);
+        a.bias[i] = (uint32_t)m << 20;  // hi + bias >= 0 for |hi| <= 2^20
     }
     a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
     a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
+    a.xwork = d_xwork;
+    RKB_CHECK_ARG(d_xwork != nullptr && d_zcount != nullptr, "the row workspace and Z counts are required");
+    RKB_CHECK_ARG(bits <= 40, "the residue path handles |x| <= 2^40 (bits <= 40)");
+    RKB_CHECK_ARG(kpad % 16 == 0, "kpad must be a multiple of 16");
+    const long np = ((long)nv * ng + 1) & ~1L, nvp = ((long)nv + 1) & ~1L;
+    const size_t per_warp = (size_t)(np + nvp) * sizeof(double);
     const int warps = 4;
-    size_t smem = (size_t)warps * ((long)nv * ng + nv) * sizeof(double);
+    size_t smem = (size_t)warps * per_warp;
     RKB_CHECK_ARG(smem <= 200 * 1024, "grid too large for the split row kernel");
     dim3 grid((unsigned)ceil_div(nrows, warps)), block(32 * warps);
     cudaStream_t st = as_stream(stream);
+    RKB_CHECK_ARG(((uintptr_t)d_resA % 16) == 0 && (d_resB == nullptr || ((uintptr_t)d_resB % 16) == 0),
+                  "residue buffers must be 16-byte aligned");
 #define RKB_SR_CASE(NGV)                                                                              \
     case NGV: {                                                                                       \
         RKB_CUDA(cudaFuncSetAttribute(split_rows_kernel<NGV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
@@ -684,18 +762,23 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
     }
 #undef RKB_SR_CASE
     RKB_LAUNCHED("split_rows_kernel");
+    const long nthreads = nrows * (kpad / 16);
+    split_residues_kernel<<<(unsigned)ceil_div(nthreads, 256), 256, 0, st>>>(a, d_zcount);
+    RKB_LAUNCHED("split_residues_kernel");
     return RKB_OK;
 }
 
 extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, long kpad,
-                                  long nrows_total, int n_mod, const int *moduli, const double *f_hi,
+                                  long nrows_total, int n_mod, const int *moduli, const int *pair_inv,
+                                  const double *f_hi,
                                   const double *f_lo, double M, const double *d_rowscale, const double *d_left,
                                   const double *d_right, const double *d_cbound, double corr_floor, int cw,
                                   int cwp, const long *d_grp_row0,
                                   const long *d_grp_n, const long *d_grp_kdim, const long *d_grp_out,
                                   const int *d_tasks, long n_tasks, double *d_out, int *d_status, void *stream) {
     RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
-    RKB_CHECK_ARG(kpad % BKB == 0 && kpad > 0, "kpad must be a positive multiple of %d", BKB);
+    RKB_CHECK_ARG(kpad % BKB == 0 && kpad > 0 && kpad <= 3456, "kpad must be a positive multiple of %d, <= 3456",
+                  BKB);
     RKB_CHECK_ARG((long)n_mod * nrows_total < (1L << 31), "residue matrices too tall for 32-bit TMA rows");
     RKB_CHECK_ARG(d_status != nullptr, "a device status word is required");
     RKB_CHECK_ARG(cw <= cwp, "cw must be <= cwp");
@@ -712,12 +795,17 @@ extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *
     p.grp_row0 = d_grp_row0; p.grp_n = d_grp_n; p.grp_kdim = d_grp_kdim; p.grp_out = d_grp_out;
     p.tasks = d_tasks; p.n_tasks = n_tasks; p.nrows_total = nrows_total; p.out = d_out; p.status = d_status;
     p.n_mod = n_mod; p.M = M;
+    const int ndig = (n_mod + 1) / 2;
     for (int i = 0; i < MAXMOD; ++i) {
-        p.mod[i] = i < n_mod ? moduli[i] : 1;
-        p.inv_mod[i] = 1.0f / (float)p.mod[i];
-        p.f_hi[i] = i < n_mod ? f_hi[i] : 0.0;
-        p.f_lo[i] = i < n_mod ? f_lo[i] : 0.0;
+        const int m = i < n_mod ? moduli[i] : 256;
+        RKB_CHECK_ARG(m >= 2 && m <= 256, "moduli must lie in [2, 256]");
+        p.mod[i] = m;
+        p.magic[i] = (uint32_t)((1ULL << 32) / (unsigned long long)m + 1ULL);
+        p.bias[i] = (uint32_t)m << 18;
+        p.f_hi[i] = i < ndig ? f_hi[i] : 0.0;
+        p.f_lo[i] = i < ndig ? f_lo[i] : 0.0;
     }
+    for (int i = 0; i < MAXMOD / 2; ++i) p.pinv[i] = i < n_mod / 2 ? (uint32_t)pair_inv[i] : 1u;
     long grid = n_tasks < sm_count() ? n_tasks : sm_count();
     cudaStream_t st = as_stream(stream);
 #define RKB_CRT_CASE(NM)                                                                                     \

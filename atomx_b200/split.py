@@ -88,7 +88,7 @@ class SplitEngine:
         self.kdim = {k: _round_up(self.kbody + self.nz[k], self.KCHUNK) for k in plan.ks}
         self.kpad = max(self.kdim.values())
         self.n_mod = int(n_mod) if n_mod is not None else moduli_needed(self.bits, self.kpad)
-        self.moduli, self.f_hi, self.f_lo, self.M = crt_constants(self.n_mod)
+        self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
         self.cw = ng
         self.cwp = _round_up(self.cw, 2)
         nrows = plan.n_rows
@@ -101,6 +101,12 @@ class SplitEngine:
         self.left = torch.empty((nrows, self.cwp), dtype=torch.float64, device=d)
         self.right = torch.empty_like(self.left)
         self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
+        # scratch: the FP64 rows [X | Z] before they are rounded to residues
+        self.xwork = torch.empty((nrows, self.kpad), dtype=torch.float64, device=d)
+        zc = np.zeros(kmax + 1, dtype=np.int32)
+        for k in plan.ks:
+            zc[k] = self.nz[k]
+        self.zcount = torch.as_tensor(zc, device=d)
         #: skip the FP64 core correction of a block when its bound is below
         #: 2^-(bits+10) of the block's scale (none of the entries can move by
         #: more than that; the split's own error is ~2^-bits of the same scale)
@@ -120,9 +126,10 @@ class SplitEngine:
         self.out = torch.empty(self.total, dtype=torch.float64, device=d)
         self._mod_c = (np.ctypeslib.as_ctypes(np.ascontiguousarray(self.moduli, dtype=np.int32)),
                        np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_hi)),
-                       np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_lo)))
+                       np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_lo)),
+                       np.ctypeslib.as_ctypes(np.ascontiguousarray(np.concatenate([self.pair_inv, [1]]).astype(np.int32))))
 
-    launches_per_step = 2
+    launches_per_step = 3
     dominant_kernel = "split::crt_syrk_kernel"
 
     def rows(self, stream=None) -> None:
@@ -134,14 +141,16 @@ class SplitEngine:
                                        self.koff.data_ptr(), self.bits, self.n_mod, self._mod_c[0],
                                        self.resA.data_ptr(), _native.ptr(self.resB), self.kpad, 0, self.rows_alloc,
                                        self.rowscale.data_ptr(), self.left.data_ptr(), self.right.data_ptr(),
-                                       self.cbound.data_ptr(), self.cwp, _native.stream_handle(stream)),
+                                       self.cbound.data_ptr(), self.cwp, self.xwork.data_ptr(),
+                                       self.zcount.data_ptr(), _native.stream_handle(stream)),
                       "rkb_split_rows")
 
     def contract(self, stream=None) -> None:
         L = _native.load()
         plan = self.dev.plan
         _native.check(L.rkb_split_contract(self.resA.data_ptr(), _native.ptr(self.resB), self.kpad, self.rows_alloc,
-                                           self.n_mod, self._mod_c[0], self._mod_c[1], self._mod_c[2], self.M,
+                                           self.n_mod, self._mod_c[0], self._mod_c[3], self._mod_c[1], self._mod_c[2],
+                                           self.M,
                                            self.rowscale.data_ptr(), self.left.data_ptr(), self.right.data_ptr(),
                                            self.cbound.data_ptr(), self.corr_floor, self.cw, self.cwp,
                                            self.grp_row0.data_ptr(), self.grp_n.data_ptr(),

@@ -40,10 +40,14 @@ Schwarz scale of every entry, which is what the split engine needs.
 CRT constants
 -------------
 Pairwise-coprime moduli m_i <= 256 (int8 residues in [-128, 127]), M = prod m_i.
-An integer x with |x| < M/2 is rebuilt from residues r_i as
-x = M * frac(sum_i r_i f_i), f_i = (M/m_i) [(M/m_i)^-1 mod m_i] / M mod 1.
-f_i is split into f_hi (a multiple of 2^-42) and f_lo = f_i - f_hi so that
-sum r_i f_hi is exact in one double for |r_i| <= 128 and up to 12 moduli.
+The device reduces each int32 accumulator to r_i in [0, m_i) and merges the
+residues of consecutive moduli into one digit d_p = r_2p + m_2p t,
+t = (r_2p+1 - r_2p) m_2p^-1 mod m_2p+1, a residue mod D_p = m_2p m_2p+1
+(< 2^16); an odd last modulus stays a digit of its own.  An integer x with
+|x| < M/2 is rebuilt from the digits as x = M * frac(sum_p d_p f_p),
+f_p = (M/D_p) [(M/D_p)^-1 mod D_p] / M mod 1.  f_p is split into f_hi (a
+multiple of 2^-34) and f_lo = f_p - f_hi, so sum d_p f_hi is exact in one
+double for up to 6 digits below 2^16.
 """
 from __future__ import annotations
 
@@ -55,7 +59,8 @@ import numpy as np
 
 from .yk import yk_partial_matrices
 
-__all__ = ["MODULI", "crt_constants", "moduli_needed", "green_factor", "pack_factors", "factor_table_layout"]
+__all__ = ["MODULI", "crt_constants", "digit_moduli", "moduli_needed", "green_factor", "pack_factors",
+           "factor_table_layout"]
 
 #: Pairwise-coprime moduli, largest first (256 = 2^8; 255 = 3*5*17; 253 = 11*23;
 #: 247 = 13*19; 217 = 7*31; the rest are primes).
@@ -74,22 +79,37 @@ def moduli_needed(bits: int, kdim: int) -> int:
     raise ValueError(f"{bits}-bit splits of length {kdim} need more than {MAX_MODULI} int8 moduli")
 
 
+def digit_moduli(n_mod: int) -> list[int]:
+    """Moduli of the merged digits: m_0 m_1, m_2 m_3, ... (+ the odd last one)."""
+    ms = MODULI[:n_mod]
+    out = [ms[i] * ms[i + 1] for i in range(0, n_mod - 1, 2)]
+    if n_mod % 2:
+        out.append(ms[-1])
+    return out
+
+
 @lru_cache(maxsize=16)
 def crt_constants(n_mod: int):
-    """(moduli, f_hi, f_lo, M as double) for the first n_mod moduli."""
+    """(moduli, f_hi, f_lo, M as double, pair inverses) for the first n_mod moduli.
+
+    f_hi / f_lo are per merged digit (see the module docstring); pair_inv[p] is
+    m_2p^-1 mod m_2p+1.
+    """
     if not 1 <= n_mod <= MAX_MODULI:
         raise ValueError("1..12 moduli supported")
     ms = MODULI[:n_mod]
     M = math.prod(ms)
     f_hi, f_lo = [], []
-    for m in ms:
-        Mi = M // m
-        inv = pow(Mi % m, -1, m)
+    for D in digit_moduli(n_mod):
+        Mi = M // D
+        inv = pow(Mi % D, -1, D)
         f = Fraction((Mi * inv) % M, M)
-        hi = Fraction(round(f * (1 << 42)), 1 << 42)
-        f_hi.append(float(hi))          # exact: a multiple of 2^-42 below 1
+        hi = Fraction(round(f * (1 << 34)), 1 << 34)
+        f_hi.append(float(hi))          # exact: a multiple of 2^-34 below 1
         f_lo.append(float(f - hi))
-    return (np.asarray(ms, dtype=np.int32), np.asarray(f_hi), np.asarray(f_lo), float(M))
+    pair_inv = [pow(ms[i], -1, ms[i + 1]) for i in range(0, n_mod - 1, 2)]
+    return (np.asarray(ms, dtype=np.int32), np.asarray(f_hi), np.asarray(f_lo), float(M),
+            np.asarray(pair_inv, dtype=np.int32))
 
 
 def green_factor(r_flat: np.ndarray, ng: int, k: int, tau: float = 1e-3) -> dict:

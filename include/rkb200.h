@@ -137,8 +137,10 @@ int rkb_table_contract_fp64(const double *d_g, const double *d_y, long ld, long 
  *
  * rkb_split_contract: for every task (group, tile_i, tile_j >= tile_i) the
  * 128 x 128 tile of R_g is computed as n_mod residue GEMMs of length
- * d_grp_kdim[g] (multiple of 128) on the tensor cores, CRT-recombined in FP64
- * with the host constants f_hi/f_lo/M, scaled and corrected, and written (and
+ * d_grp_kdim[g] (multiple of 128, <= 3456) on the tensor cores, CRT-recombined
+ * in FP64 from digits merged over consecutive moduli pairs with the HOST
+ * constants pair_inv (m_2p^-1 mod m_2p+1) and per-digit f_hi/f_lo/M (see
+ * atomx_b200/split_plan.py), scaled and corrected, and written (and
  * mirrored) into the n x n block at d_out + d_grp_out[g], as
  * rkb_table_contract_fp64 does.  The FP64 core correction of a 32 x 64 block
  * is skipped when its bound from d_cbound (relative to 2^(e_a + e_b), which
@@ -151,10 +153,12 @@ int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_ld, const lo
                    int nv, int ng, const double *d_ktab, const long *d_koff, int bits, int n_mod,
                    const int *moduli, signed char *d_resA, signed char *d_resB, long kpad,
                    long row_base, long nrows_total, double *d_rowscale, double *d_left,
-                   double *d_right, double *d_cbound, int cwp, void *stream);
+                   double *d_right, double *d_cbound, int cwp, double *d_xwork,
+                   const int *d_zcount, void *stream);
 
 int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, long kpad,
-                       long nrows_total, int n_mod, const int *moduli, const double *f_hi,
+                       long nrows_total, int n_mod, const int *moduli, const int *pair_inv,
+                       const double *f_hi,
                        const double *f_lo, double M, const double *d_rowscale,
                        const double *d_left, const double *d_right, const double *d_cbound,
                        double corr_floor, int cw, int cwp,

@@ -54,12 +54,27 @@ def residues(xq, moduli):
     return out
 
 
-def crt_value(res_list, moduli, f_hi, f_lo, M):
-    yh = np.zeros(res_list[0].shape)
-    yl = np.zeros(res_list[0].shape)
-    for r, fh, fl in zip(res_list, f_hi, f_lo):
-        yh = yh + r * fh
-        yl = yl + r * fl
+def merge_digits(res_list, moduli, pair_inv):
+    """[0, m) residues -> merged digits exactly as the device merges them."""
+    rs = [np.mod(np.asarray(r, dtype=np.int64), int(m)) for r, m in zip(res_list, moduli)]
+    out = []
+    for p in range(len(moduli) // 2):
+        re, ro = rs[2 * p], rs[2 * p + 1]
+        me, mo = int(moduli[2 * p]), int(moduli[2 * p + 1])
+        t = np.mod((ro + 2 * mo - re) * int(pair_inv[p]), mo)
+        out.append(re + me * t)
+    if len(moduli) % 2:
+        out.append(rs[-1])
+    return out
+
+
+def crt_value(res_list, moduli, f_hi, f_lo, M, pair_inv):
+    digits = merge_digits(res_list, moduli, pair_inv)
+    yh = np.zeros(digits[0].shape)
+    yl = np.zeros(digits[0].shape)
+    for d, fh, fl in zip(digits, f_hi, f_lo):
+        yh = yh + d * fh
+        yl = yl + d * fl
     return (yh - np.rint(yh)) * M + yl * M
 
 
@@ -89,10 +104,10 @@ def reduce_mod(v, m):
     return r
 
 
-def emulate_table(Ares, Bres, rowscale, left, right, moduli, f_hi, f_lo, M):
+def emulate_table(Ares, Bres, rowscale, left, right, moduli, f_hi, f_lo, M, pair_inv):
     """One symmetric table from residue rows (lists per modulus of (n, K))."""
     res = []
     for a, b, m in zip(Ares, Bres, moduli):
         res.append(reduce_mod(a.astype(np.int64) @ b.astype(np.int64).T, int(m)))
-    x = crt_value(res, moduli, f_hi, f_lo, M)
+    x = crt_value(res, moduli, f_hi, f_lo, M, pair_inv)
     return x * np.outer(rowscale, rowscale) + left @ right.T

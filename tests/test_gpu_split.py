@@ -101,7 +101,7 @@ def _tile_check(eng, k, ti, tj):
     from split_emulation import reduce_mod
     for a, b, m in zip(Ai, Bj, eng.moduli):
         res.append(reduce_mod(a.astype(np.int64) @ b.astype(np.int64).T, int(m)))
-    x = crt_value(res, eng.moduli, eng.f_hi, eng.f_lo, eng.M)
+    x = crt_value(res, eng.moduli, eng.f_hi, eng.f_lo, eng.M, eng.pair_inv)
     ref = x * np.outer(rs[off + ri], rs[off + rj]) + lf[off + ri] @ rt[off + rj].T
     T = eng.out[eng.offsets[k]:eng.offsets[k] + nk * nk].view(nk, nk).cpu().numpy()
     got = T[np.ix_(ri, rj)]

@@ -49,7 +49,7 @@ def test_crt_constants_reconstruct_integers():
     from atomx_b200.split_plan import crt_constants, moduli_needed
     for bits, kdim in ((36, 896), (36, 2176), (40, 1024)):
         nm = moduli_needed(bits, kdim)
-        ms, fh, fl, M = crt_constants(nm)
+        ms, fh, fl, M, pinv = crt_constants(nm)
         assert M > 2 * kdim * 2.0 ** (2 * bits)
         rng = np.random.default_rng(bits)
         bound = kdim * 2 ** (2 * bits)
@@ -57,10 +57,10 @@ def test_crt_constants_reconstruct_integers():
         xs = [x % (2 * bound) - bound for x in xs]
         for x in xs:
             res = [np.array([((x + int(m) // 2) % int(m)) - int(m) // 2]) for m in ms]  # any representative
-            got = float(crt_value(res, ms, fh, fl, M)[0])
+            got = float(crt_value(res, ms, fh, fl, M, pinv)[0])
             assert abs(got - float(x)) <= 2.0 ** -50 * abs(float(x)) + 8.0, (bits, x, got)
-        # f_hi exactness: multiples of 2^-42
-        assert np.all(fh * 2.0 ** 42 == np.rint(fh * 2.0 ** 42))
+        # f_hi exactness: multiples of 2^-34
+        assert np.all(fh * 2.0 ** 34 == np.rint(fh * 2.0 ** 34))
 
 
 def test_fixed_point_split_error_model():
