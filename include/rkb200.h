@@ -132,7 +132,11 @@ int rkb_table_contract_fp64(const double *d_g, const double *d_y, long ld, long 
  * core correction vectors (width cwp >= ng) left = g_0, right = S_c g_0 to
  * d_left / d_right, and to d_cbound[2q], d_cbound[2q+1] the norms |g_0| and
  * |S_c g_0| divided by 2^e_q (>= the row maximum of |[X | Z]|).  d_ktab holds the
- * per-k factor tables at offsets d_koff[k] (layout in atomx_b200/split_plan.py).
+ * per-k factor tables at offsets d_koff[k] (layout in atomx_b200/split_plan.py)
+ * and d_zcount[k] their Z-column counts.  d_xwork is caller-provided scratch
+ * of (row_base + nrows) x kpad doubles that receives the FP64 rows [X | Z | 0]
+ * before they are rounded.  A row with a non-finite value gets a NaN scale
+ * and zero residues, so every entry it reaches comes out NaN.
  * `moduli` is a HOST array of n_mod pairwise-coprime ints <= 256.
  *
  * rkb_split_contract: for every task (group, tile_i, tile_j >= tile_i) the
