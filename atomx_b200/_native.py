@@ -33,6 +33,8 @@ _SIGNATURES = {
     "rkb_table_contract_fp64": [_vp, _vp, _l, _l, _vp, _vp, _vp, _vp, _l, _vp, _vp],
     "rkb_split_rows": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _l, _l,
                        _l, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
+    "rkb_split_rows_noalloc": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _l,
+                               _l, _l, _vp, _vp, _vp, _vp, _i, _vp, _vp],
     "rkb_split_contract": [_vp, _vp, _l, _l, _i, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp,
                            _vp, _vp, _vp, _l, _vp, _vp, _vp],
 }

@@ -30,6 +30,8 @@
 //      RKB_ETIMEDOUT in *status and every role drains and returns.
 #include <cuda.h>
 
+#include <mutex>
+
 #include "rkb_common.cuh"
 
 namespace rkb {
@@ -825,4 +827,62 @@ extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *
 #undef RKB_CRT_CASE
     RKB_LAUNCHED("crt_syrk_kernel");
     return RKB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// rkb_split_rows_noalloc: rkb_split_rows whose row workspace is a fixed array
+// compiled into this library instead of caller memory.  It is meant for hosts
+// that cannot call cudaMalloc on this path: a C or Fortran program that links
+// only this ABI and hands over buffers from its own pool, or a process that
+// plans every device allocation up front and may not have cudaMalloc /
+// cudaFree synchronise the device in the middle of its pipelined streams.
+//
+// The array holds RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES doubles (16 MiB) on every
+// GPU that loads the library, until the process exits.  The host name of a
+// __device__ array is only a host-side stand-in, so its device address is
+// looked up per device with cudaGetSymbolAddress, on the first call made with
+// that device current; make that first call before any stream capture.
+// Every call shares the one array, so calls that overlap on the GPU (other
+// streams, other host threads) race and must be serialised by the caller.
+// Nothing needs clearing between calls: the row kernel writes every element
+// of each row [X | Z | 0] that the residue kernel later reads.
+namespace rkb {
+namespace split {
+static __device__ __align__(256) double g_noalloc_xwork[RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static double *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_noalloc_mutex;
+}  // namespace split
+}  // namespace rkb
+
+extern "C" int rkb_split_rows_noalloc(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                                      const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                                      int nv, int ng, const double *d_ktab, const long *d_koff, int bits,
+                                      int n_mod, const int *moduli, signed char *d_resA, signed char *d_resB,
+                                      long kpad, long row_base, long nrows_total, double *d_rowscale,
+                                      double *d_left, double *d_right, double *d_cbound, int cwp,
+                                      const int *d_zcount, void *stream) {
+    const long cap = (long)RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES;
+    RKB_CHECK_ARG(kpad > 0 && nrows >= 0 && row_base >= 0, "invalid row range or width");
+    RKB_CHECK_ARG(row_base <= cap / kpad && nrows <= cap / kpad - row_base,
+                  "rows [0, %ld) of width %ld need %ld workspace doubles; the fixed workspace holds %ld "
+                  "(use rkb_split_rows with a caller buffer)",
+                  row_base + nrows, kpad, (row_base + nrows) * kpad, cap);
+    int dev = -1;
+    RKB_CUDA(cudaGetDevice(&dev));
+    RKB_CHECK_ARG(dev >= 0 && dev < NOALLOC_MAX_DEVICES, "device ordinal %d out of range", dev);
+    double *ws = nullptr;
+    {
+        std::lock_guard<std::mutex> guard(g_noalloc_mutex);
+        if (g_noalloc_addr[dev] == nullptr) {
+            void *addr = nullptr;
+            RKB_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_xwork));
+            g_noalloc_addr[dev] = static_cast<double *>(addr);
+        }
+        ws = g_noalloc_addr[dev];
+    }
+    return rkb_split_rows(d_Pv, d_Qv, orb_ld, d_pairs, d_row_pair, d_row_k, nrows, d_w, nv, ng, d_ktab, d_koff,
+                          bits, n_mod, moduli, d_resA, d_resB, kpad, row_base, nrows_total, d_rowscale, d_left,
+                          d_right, d_cbound, cwp, ws, d_zcount, stream);
 }

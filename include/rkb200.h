@@ -170,6 +170,32 @@ int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, lon
                        const long *d_grp_out, const int *d_tasks, long n_tasks, double *d_out,
                        int *d_status, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * rkb_split_rows_noalloc: no counterpart in the reference (an addition of this
+ * library).  The same computation and arguments as rkb_split_rows, without
+ * d_xwork: the FP64 row workspace is a fixed device array inside the library,
+ * so the call allocates no device memory.  For hosts that cannot allocate on
+ * this path (a C or Fortran program with its own device pool that links only
+ * this ABI; a process that plans all device memory up front and cannot let
+ * cudaMalloc / cudaFree synchronise the device mid-pipeline).
+ *
+ * Limit: (row_base + nrows) * kpad <= RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES
+ * (16 MiB of doubles, held on every GPU that loads the library until exit);
+ * larger requests return RKB_EINVAL.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race, so serialise them.
+ * ------------------------------------------------------------------------- */
+#define RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES (2L * 1024L * 1024L)
+
+int rkb_split_rows_noalloc(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                           const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                           int nv, int ng, const double *d_ktab, const long *d_koff, int bits, int n_mod,
+                           const int *moduli, signed char *d_resA, signed char *d_resB, long kpad,
+                           long row_base, long nrows_total, double *d_rowscale, double *d_left,
+                           double *d_right, double *d_cbound, int cwp, const int *d_zcount,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif
