@@ -7,7 +7,7 @@ order-9 B-splines on [1e-6, 60] bohr with 8 Gauss nodes per cell (N = 896),
 the ``e2e`` leg starts from host coefficient arrays and ends with the whole
 table in pinned host memory.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--engine split|fp64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--engine split|fp64] [--k-max K]
     python bench.py --impl reference   # the reference algorithm on host cores
 
 Multi-GPU: one process per GPU (torchrun); each rank computes its own ion
@@ -218,6 +218,102 @@ def l2_flush(buf):
     buf.zero_()
 
 
+def _fp64_engine(dev, stream):
+    """Plain FP64 engine: (step, out, workspace)."""
+    import torch
+
+    from atomx_b200 import tables as T
+    ws = T.Fp64Workspace(dev)
+    out = torch.empty(ws.total, device="cuda", dtype=torch.float64)
+
+    def step():
+        T.run_fp64(dev, ws, out, stream=stream)
+        return out
+
+    return step, out, ws
+
+
+def _time_steps(step, n, flush, stream):
+    """Device time (ms) of n steps, each after an L2 flush, CUDA events on stream."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+    for a, b in ev:
+        l2_flush(flush)
+        a.record(stream)
+        step()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
+
+
+def _fp64_roofline(dev, ws, out, stream, flush):
+    """Dominant FP64 kernel (the table contraction) alone, CUDA events on stream."""
+    import torch
+
+    from atomx_b200 import _native
+    L = _native.load()
+    plan = dev.plan
+    s = _native.stream_handle(stream)
+    _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                        dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows, dev.r.data_ptr(),
+                                        dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(), dev.mi.data_ptr(),
+                                        ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, s), "rkb_table_rows_fp64")
+
+    def contract():
+        _native.check(L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
+                                                ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr(),
+                                                ws.n_tasks, out.data_ptr(), s), "rkb_table_contract_fp64")
+
+    kms = statistics.median(_time_steps(contract, 3, flush, stream))
+    # algorithmic flops: 2*N per unique entry (i <= j) of every table
+    flops = 2.0 * dev.n * plan.unique_entries
+    peak_tf, src = fp64_peak()
+    ach = flops / (kms / 1e3) / 1e12
+    return {"bound": "tensor", "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s", "frac": ach / peak_tf,
+            "traffic": profiled_traffic("fp64tab::contract_kernel", dev.plan), "kernel": "fp64tab::contract_kernel",
+            "kernel_ms": kms, "peak_source": src, "algorithmic_flops": flops, "unit_of_work": "unique entry",
+            "units_per_launch": int(plan.unique_entries)}
+
+
+def table_errors(test, ref, offsets, plan):
+    """Errors of a whole table against the FP64 table, per k block.
+
+    schwarz: |x - ref| / sqrt(|ref_ii| |ref_jj|) (the Cauchy-Schwarz scale of
+    the entry); floored: |x - ref| / max(|ref|, 1e-6 max|ref| of the k table);
+    abs: max |x - ref|.
+    """
+    import torch
+    schwarz = floored = absmax = 0.0
+    for k in plan.ks:
+        nk = plan.n_of_k(k)
+        o = offsets[k]
+        t = test[o:o + nk * nk].view(nk, nk)
+        r = ref[o:o + nk * nk].view(nk, nk)
+        d = (t - r).abs()
+        dg = r.diagonal().abs().sqrt()
+        scale = torch.outer(dg, dg)
+        schwarz = max(schwarz, float((d / scale).max()))
+        floor = 1e-6 * float(r.abs().max())
+        floored = max(floored, float((d / r.abs().clamp_min(floor)).max()))
+        absmax = max(absmax, float(d.max()))
+        del d, scale
+    return {"max_schwarz_rel": schwarz, "max_rel_floored_1e-6": floored, "max_abs": absmax}
+
+
+def profiled_traffic(kernel: str, plan):
+    """DRAM bytes per launch of ``kernel`` for this plan, scaled from the
+    committed ncu summary (profiles/traffic.json: bytes measured on a smaller
+    case and the units it processed); None when no summary is present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        rec = json.load(f).get(kernel)
+    if not rec:
+        return None
+    return rec["bytes"] / rec["units"] * plan.unique_entries
+
+
 def run_gpu(args):
     import torch
 
@@ -226,8 +322,9 @@ def run_gpu(args):
 
     rank, world, local = dist_setup(args.gpus)
     spec = W.ytterbium_scaleup(seed=2026 + rank)
+    k_max = spec.k_max if args.k_max is None else args.k_max
     ion = W.build_ion(spec)
-    dev = T.upload_ion(ion)
+    dev = T.upload_ion(ion, k_max=k_max)
     plan = dev.plan
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -236,93 +333,69 @@ def run_gpu(args):
     if engine == "split":
         from atomx_b200.split import SplitEngine
         eng = SplitEngine(dev)
-        out = None
 
         def step():
-            return eng.run(stream=stream, upload=False)
+            return eng.run(stream=stream, upload=False, check=False)
 
         launches_per_step = eng.launches_per_step
-        dom_name = eng.dominant_kernel
     else:
-        ws = T.Fp64Workspace(dev)
-        out = torch.empty(ws.total, device="cuda", dtype=torch.float64)
-
-        def step():
-            T.run_fp64(dev, ws, out, stream=stream)
-            return out
-
+        step, out64, ws = _fp64_engine(dev, stream)
         launches_per_step = 2
-        dom_name = "fp64tab::contract_kernel"
 
-    # warm-up
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
 
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local) as clk:
         barrier(world)
         torch.cuda.synchronize()
         t_wall = time.perf_counter()
-        for i in range(args.steps):
-            l2_flush(flush)
-            ev[i][0].record(stream)
-            step()
-            ev[i][1].record(stream)
-        torch.cuda.synchronize()
+        times = _time_steps(step, args.steps, flush, stream)
         barrier(world)
         t_wall = time.perf_counter() - t_wall
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
-    dev_ms_max = allreduce_max(dev_ms, world)
-    entries = float(plan.ordered_entries) * args.steps
-    entries_all = allreduce_sum(entries, world)
+    if engine == "split":
+        eng.check_status()
+    dev_ms_max = allreduce_max(sum(times), world)
+    entries_all = allreduce_sum(float(plan.ordered_entries) * args.steps, world)
     value = entries_all / (dev_ms_max / 1e3)
 
-    # dominant kernel alone (same stream, same events), for the roofline
-    dom = {}
-    if engine == "fp64":
-        k_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(3)]
-        from atomx_b200 import _native
-        L = _native.load()
-        s = _native.stream_handle(stream)
-        L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
-                              dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows, dev.r.data_ptr(),
-                              dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(), dev.mi.data_ptr(),
-                              ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, s)
-        for a, b in k_ev:
-            l2_flush(flush)
-            a.record(stream)
-            L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
-                                      ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr(), ws.n_tasks,
-                                      out.data_ptr(), s)
-            b.record(stream)
-        torch.cuda.synchronize()
-        kms = statistics.median(a.elapsed_time(b) for a, b in k_ev)
-        # algorithmic flops per launch: 2*N per computed entry (upper tiles incl. diagonal tiles)
-        computed = sum(min(128, plan.n_of_k(kk) - ti * 128) * min(128, plan.n_of_k(kk) - tj * 128)
-                       for kk in plan.ks for (g, ti, tj) in [(0, a_, b_) for a_ in range((plan.n_of_k(kk) + 127) // 128)
-                                                             for b_ in range(a_, (plan.n_of_k(kk) + 127) // 128)])
-        flops = 2.0 * dev.n * computed
-        peak_tf, src = fp64_peak()
-        dom = {"bound": "tensor", "achieved": flops / (kms / 1e3) / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
-               "frac": flops / (kms / 1e3) / 1e12 / peak_tf, "traffic": None, "kernel": dom_name,
-               "kernel_ms": kms, "peak_source": src, "algorithmic_flops": flops}
-    else:
+    extra = {}
+    if engine == "split":
         dom = eng.roofline(stream=stream, flush=flush)
+        dom["traffic"] = profiled_traffic(dom["kernel"], plan)
+        if not args.no_compare:
+            # the plain FP64 engine on the same ion: its speed and the split error
+            step64, out64, ws = _fp64_engine(dev, stream)
+            for _ in range(3):
+                step64()
+            t64 = _time_steps(step64, max(2, min(args.steps, 5)), flush, stream)
+            ms64 = allreduce_max(statistics.mean(t64), world)
+            split_out = eng.run(stream=stream, check=True)
+            torch.cuda.synchronize()
+            err = table_errors(split_out, out64, eng.offsets, plan)
+            gate = 1e-10
+            extra["fp64_engine"] = {"ms_per_step": ms64, "value": float(plan.ordered_entries) * world / (ms64 / 1e3),
+                                    "speedup_split_vs_fp64": ms64 / (dev_ms_max / args.steps)}
+            extra["error_vs_fp64"] = dict(err, gate_schwarz_rel=gate, within_gate=err["max_schwarz_rel"] <= gate)
+            del out64, ws
+        extra["split"] = eng.info()
+    else:
+        dom = _fp64_roofline(dev, ws, out64, stream, flush)
 
-    # e2e through the public API with host buffers
-    e2e = e2e_leg(ion, engine, args, world)
+    e2e = None if args.no_e2e else e2e_leg(ion, engine, args, world, k_max)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if engine == "fp64" else "i8",
             "data": "synthetic (seeded Dirac-Coulomb spinors, no external dataset)",
-            "config": {"workload": WORKLOAD, "engine": engine, "entries_per_step": plan.ordered_entries,
+            "config": {"workload": WORKLOAD if k_max == spec.k_max else f"{WORKLOAD} (k<={k_max} subset)",
+                       "engine": engine, "k_max": k_max, "entries_per_step": plan.ordered_entries,
                        "unique_entries_per_step": plan.unique_entries, "rows": plan.n_rows,
                        "l2": "256 MiB flush between timed steps; working set > L2",
                        "parallelism": f"replicas x{world} (independent ions, no collective)"},
             "roofline": dom, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(), "wall_s": t_wall}
+    line.update(extra)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
@@ -354,7 +427,7 @@ def fp64_peak():
     return 2.0 * n ** 3 / best / 1e12, "measured here: cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 3"
 
 
-def e2e_leg(ion, engine, args, world):
+def e2e_leg(ion, engine, args, world, k_max):
     """Same metric through the public API from host arrays to a host table."""
     import torch
 
@@ -367,7 +440,7 @@ def e2e_leg(ion, engine, args, world):
     for i in range(steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        tab = T.slater_rk_tables(ion, precision=engine)
+        tab = T.slater_rk_tables(ion, k_max=k_max, precision=engine)
         if host_out is None:
             host_out = torch.empty(tab.values.numel(), dtype=torch.float64, pin_memory=True)
         host_out.copy_(tab.values, non_blocking=True)
@@ -391,8 +464,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--engine", default=os.environ.get("RKB_ENGINE", "fp64"), choices=["split", "fp64"])
+    ap.add_argument("--engine", default=os.environ.get("RKB_ENGINE", "split"), choices=["split", "fp64"])
+    ap.add_argument("--k-max", type=int, default=None, help="multipole cut (default: the workload's 12)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
