@@ -55,6 +55,7 @@ struct RowsArgs {
     int bits, n_mod;
     int mod[MAXMOD];
     uint32_t magic[MAXMOD], c20[MAXMOD], bias[MAXMOD];  // 2^32/m + 1, 2^20 mod m, m * 2^20
+    double inv_mod[MAXMOD];    // RN(1/m)
     signed char *resA, *resB;  // [n_mod][nrows_total][kpad]; resB may be null
     long kpad, row_base, nrows_total;
     double *rowscale, *left, *right, *cbound;
@@ -277,6 +278,197 @@ __global__ void __launch_bounds__(256) split_residues_kernel(RowsArgs a, const i
         const long o = ((long)md * a.nrows_total + grow) * a.kpad + c0;
         *reinterpret_cast<uint4 *>(a.resA + o) = make_uint4(w[0], w[1], w[2], w[3]);
         if (a.resB) *reinterpret_cast<uint4 *>(a.resB + o) = make_uint4(wb[0], wb[1], wb[2], wb[3]);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Fused row kernel (rows whose body fits in registers): one warp per row, no
+// shared memory and no FP64 workspace.  Cells are taken from the last to the
+// first in passes of CPP = 32/NG cells (lane = (cell offset, node)), so the
+// suffix sums t_m = sum_{m'>m} u_m'.g_m' are a running carry; each lane keeps
+// its X value of every pass in registers until the row maximum is known, then
+// writes int8 residues directly.
+//
+// Residue layout (any column order shared by every row of a GEMM leaves the
+// products unchanged): the value of pass p held by lane l goes to position
+// 128*(p/4) + 4*l + (p%4), so four passes form one 32-bit word per lane and a
+// warp stores 128 contiguous bytes per modulus.  Lanes without a cell (l >=
+// CPP*NG, or cell 0 / below in the last pass) hold zeros.  The body therefore
+// spans fused_body_width() positions; Z column e sits at body_width + e.
+__host__ __device__ constexpr int fused_cpp(int ng) { return 32 / ng; }
+__host__ __device__ inline long fused_passes(int nv, int ng) { return (nv - 1 + fused_cpp(ng) - 1) / fused_cpp(ng); }
+__host__ __device__ inline long fused_body_width(int nv, int ng) { return 128 * ((fused_passes(nv, ng) + 3) / 4); }
+constexpr int FUSED_PMAX = 32;  // passes kept in registers (body width <= 1024)
+constexpr int FUSED_ZMAX = 64;  // Z columns per row (two per lane)
+
+// Centred residue of an integer-valued double |x| <= 2^40 modulo m <= 256:
+// q = round(x/m) with the 1.5*2^52 rounding constant (x*inv_m is within
+// 2^-13 of x/m, and x/m is never that close to a half-integer except exactly
+// at one, where either rounding is fine), r = x - q*m exactly by one fma,
+// |r| <= m/2, then moved into [-128, 127].
+__device__ __forceinline__ uint32_t residue_f64(double x, double m, double inv_m) {
+    const double rc = 6755399441055744.0;  // 1.5 * 2^52
+    const double q = __dadd_rn(__fma_rn(x, inv_m, rc), -rc);
+    const double r = __fma_rn(-q, m, x);
+    int ri = __double2loint(__dadd_rn(r, rc));
+    ri -= ri > 127 ? (int)m : 0;
+    return (uint32_t)ri & 0xffu;
+}
+
+template <int NG>
+__global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
+    constexpr int CPP = 32 / NG;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int nv = a.nv;
+    const int lane = threadIdx.x & 31;
+    const long q = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (q >= a.nrows) return;
+    const int k = a.row_k[q];
+    const long pr = a.row_pair[q];
+    const double *Pa = a.P + a.pairs[2 * pr] * a.orb_ld, *Pc = a.P + a.pairs[2 * pr + 1] * a.orb_ld;
+    const double *Qa = a.Q + a.pairs[2 * pr] * a.orb_ld, *Qc = a.Q + a.pairs[2 * pr + 1] * a.orb_ld;
+    const long n = (long)nv * NG;
+    const double *tab = a.ktab + a.koff[k];
+    const double *u = tab;
+    const double *ell = u + n;
+    const double *Lb = ell + n;
+    const double *C = Lb + (long)nv * NG * NG;
+    const double *v0 = C + (long)nv * NG;
+    const double *Sc = v0 + NG;
+    const int nz = (int)Sc[NG * NG];
+    const double *zt = Sc + NG * NG + 1;
+    const int sub = lane / NG, node = lane - sub * NG;
+    const bool glane = sub < CPP;
+    const long grow = a.row_base + q;
+    auto gval = [&](long i) {
+        return __dmul_rn(a.w[i], __dadd_rn(__dmul_rn(Pa[i], Pc[i]), __dmul_rn(Qa[i], Qc[i])));
+    };
+
+    // cell 0: g_0 (lanes < NG), alpha = v_0 . g_0, core vectors and their norms
+    const double g0 = lane < NG ? gval(lane) : 0.0;
+    const double alpha = warp_sum(lane < NG ? v0[lane] * g0 : 0.0);
+    double sg = 0.0;
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        const double gj = __shfl_sync(FULL, g0, j);
+        if (lane < NG) sg = fma(Sc[lane * NG + j], gj, sg);
+    }
+    if (lane < a.cwp) {
+        a.left[grow * a.cwp + lane] = g0;
+        a.right[grow * a.cwp + lane] = sg;
+    }
+    const double n1 = warp_sum(g0 * g0), n2 = warp_sum(sg * sg);
+
+    // body passes, last cell first
+    const int P = (int)fused_passes(nv, NG);
+    double xs[FUSED_PMAX];
+    double carry = 0.0, amax = 0.0;
+    bool bad = false;
+#pragma unroll
+    for (int p = 0; p < FUSED_PMAX; ++p) {
+        xs[p] = 0.0;
+        if (p < P) {
+            const int m = nv - 1 - p * CPP - sub;
+            const bool ok = glane && m >= 1;
+            const long i = (long)m * NG + node;
+            const double g = ok ? gval(i) : 0.0;
+            double dm = ok ? u[i] * g : 0.0;
+            // sum over the NG lanes of the group (every lane of the group gets it)
+            {
+                double tot = 0.0;
+#pragma unroll
+                for (int t = 0; t < NG; ++t) tot += __shfl_sync(FULL, dm, (sub * NG + t) & 31);
+                dm = tot;
+            }
+            // carry of the cells already passed plus the higher cells of this pass
+            double before = 0.0, all = 0.0;
+#pragma unroll
+            for (int s = 0; s < CPP; ++s) {
+                const double ds = __shfl_sync(FULL, dm, s * NG);
+                all += ds;
+                before += s < sub ? ds : 0.0;
+            }
+            const double t = carry + before;
+            carry += all;
+            const double *L = Lb + (long)m * NG * NG;
+            double x = ok ? fma(ell[i], alpha, C[i] * t) : 0.0;
+#pragma unroll
+            for (int ii = 0; ii < NG; ++ii) {
+                const double gi = __shfl_sync(FULL, g, (sub * NG + ii) & 31);
+                if (ok && ii >= node) x = fma(L[ii * NG + node], gi, x);
+            }
+            xs[p] = x;
+            amax = fmax(amax, fabs(x));
+            bad |= !isfinite(x);
+        }
+    }
+    // Z columns: lane e and e + 32
+    double zx[2] = {0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int e = lane + 32 * h;
+        if (e < nz) {
+            const double *ze = zt + (long)e * (NG + 1);
+            const long base = (long)ze[0] * NG;
+            double x = 0.0;
+            for (int ii = 0; ii < NG; ++ii) x = fma(ze[1 + ii], gval(base + ii), x);
+            zx[h] = x;
+            amax = fmax(amax, fabs(x));
+            bad |= !isfinite(x);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(FULL, amax, o));
+    bad = __any_sync(FULL, bad);
+    int ex = 0;
+    double scale = 0.0, inv_scale = 0.0;
+    if (!bad && amax > 0.0) {
+        frexp(amax, &ex);  // amax < 2^ex
+        scale = ldexp(1.0, a.bits - ex);
+        inv_scale = ldexp(1.0, ex - a.bits);
+    }
+    if (lane == 0) {
+        a.rowscale[grow] = bad ? __longlong_as_double(0x7ff8000000000000LL) : inv_scale;
+        const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
+        a.cbound[grow * 2] = sqrt(n1) * rel;
+        a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+    }
+
+    // quantise in place (exact integers, |x| <= 2^bits) and write residues
+    const double rc = 6755399441055744.0;
+#pragma unroll
+    for (int p = 0; p < FUSED_PMAX; ++p) xs[p] = __dadd_rn(__fma_rn(xs[p], scale, rc), -rc);
+    zx[0] = __dadd_rn(__fma_rn(zx[0], scale, rc), -rc);
+    zx[1] = __dadd_rn(__fma_rn(zx[1], scale, rc), -rc);
+    const long bw = fused_body_width(nv, NG);
+    for (int md = 0; md < a.n_mod; ++md) {
+        const double m = (double)a.mod[md], inv_m = a.inv_mod[md];
+        signed char *rowA = a.resA + ((long)md * a.nrows_total + grow) * a.kpad;
+        signed char *rowB = a.resB ? a.resB + ((long)md * a.nrows_total + grow) * a.kpad : nullptr;
+#pragma unroll
+        for (int j = 0; j < FUSED_PMAX / 4; ++j) {
+            if (4 * j < P) {
+                uint32_t word = 0u;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) word |= residue_f64(xs[4 * j + s], m, inv_m) << (8 * s);
+                reinterpret_cast<uint32_t *>(rowA + 128 * j)[lane] = word;
+                if (rowB) reinterpret_cast<uint32_t *>(rowB + 128 * j)[lane] = word;
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = lane + 32 * h;
+            if (e < nz) {
+                const uint32_t r = residue_f64(zx[h], m, inv_m);
+                rowA[bw + e] = (signed char)r;
+                if (rowB) {
+                    int nr = -(int)(int8_t)(uint8_t)r;  // residue of -x, centred again
+                    nr -= nr > 127 ? (int)m : 0;
+                    rowB[bw + e] = (signed char)nr;
+                }
+            }
+        }
     }
 }
 
@@ -732,6 +924,7 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
         a.magic[i] = (uint32_t)((1ULL << 32) / (unsigned long long)m + 1ULL);
         a.c20[i] = (uint32_t)((1u << 20) % (uint32_t)m);
         a.bias[i] = (uint32_t)m << 20;  // hi + bias >= 0 for |hi| <= 2^20
+        a.inv_mod[i] = 1.0 / (double)m;
     }
     a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
     a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
@@ -767,6 +960,60 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
     const long nthreads = nrows * (kpad / 16);
     split_residues_kernel<<<(unsigned)ceil_div(nthreads, 256), 256, 0, st>>>(a, d_zcount);
     RKB_LAUNCHED("split_residues_kernel");
+    return RKB_OK;
+}
+
+extern "C" long rkb_split_fused_body_width(int nv, int ng) {
+    if (nv < 2 || ng < 1 || ng > 32) return -1;
+    return rkb::split::fused_body_width(nv, ng);
+}
+
+extern "C" int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                                    const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                                    int nv, int ng, const double *d_ktab, const long *d_koff, int max_z, int bits,
+                                    int n_mod, const int *moduli, signed char *d_resA, signed char *d_resB,
+                                    long kpad, long row_base, long nrows_total, double *d_rowscale, double *d_left,
+                                    double *d_right, double *d_cbound, int cwp, void *stream) {
+    RKB_CHECK_ARG(nv >= 2 && ng >= 5 && ng <= 11, "the fused row kernel takes 5 <= ng <= 11 (got %d)", ng);
+    RKB_CHECK_ARG(fused_passes(nv, ng) <= FUSED_PMAX, "grid too long for the fused row kernel (%ld passes > %d)",
+                  fused_passes(nv, ng), FUSED_PMAX);
+    RKB_CHECK_ARG(max_z >= 0 && max_z <= FUSED_ZMAX, "the fused row kernel takes <= %d Z columns (got %d)",
+                  FUSED_ZMAX, max_z);
+    RKB_CHECK_ARG(bits >= 8 && bits <= 40, "bits must be in [8, 40] (got %d)", bits);
+    RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
+    RKB_CHECK_ARG(kpad % BKB == 0 && kpad >= fused_body_width(nv, ng) + max_z,
+                  "kpad must be a multiple of %d >= %ld", BKB, fused_body_width(nv, ng) + max_z);
+    RKB_CHECK_ARG(cwp >= ng && cwp <= 32, "correction width must be in [ng, 32]");
+    RKB_CHECK_ARG(d_cbound != nullptr, "the correction-bound array is required");
+    RKB_CHECK_ARG(row_base >= 0 && row_base + nrows <= nrows_total, "row range outside the residue matrices");
+    RKB_CHECK_ARG(((uintptr_t)d_resA % 16) == 0 && (d_resB == nullptr || ((uintptr_t)d_resB % 16) == 0),
+                  "residue buffers must be 16-byte aligned");
+    if (nrows == 0) return RKB_OK;
+    RowsArgs a = {};
+    a.P = d_Pv; a.Q = d_Qv; a.orb_ld = orb_ld; a.pairs = d_pairs; a.row_pair = d_row_pair; a.row_k = d_row_k;
+    a.nrows = nrows; a.w = d_w; a.nv = nv; a.ng = ng; a.ktab = d_ktab; a.koff = d_koff; a.bits = bits;
+    a.n_mod = n_mod;
+    for (int i = 0; i < MAXMOD; ++i) {
+        const int m = i < n_mod ? moduli[i] : 256;
+        RKB_CHECK_ARG(m >= 2 && m <= 256, "moduli must lie in [2, 256]");
+        a.mod[i] = m;
+        a.inv_mod[i] = 1.0 / (double)m;
+    }
+    a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
+    a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
+    const int warps = 4;
+    dim3 grid((unsigned)ceil_div(nrows, warps)), block(32 * warps);
+    cudaStream_t st = as_stream(stream);
+    switch (ng) {
+        case 5: split_rows_fused_kernel<5><<<grid, block, 0, st>>>(a); break;
+        case 6: split_rows_fused_kernel<6><<<grid, block, 0, st>>>(a); break;
+        case 7: split_rows_fused_kernel<7><<<grid, block, 0, st>>>(a); break;
+        case 8: split_rows_fused_kernel<8><<<grid, block, 0, st>>>(a); break;
+        case 9: split_rows_fused_kernel<9><<<grid, block, 0, st>>>(a); break;
+        case 10: split_rows_fused_kernel<10><<<grid, block, 0, st>>>(a); break;
+        default: split_rows_fused_kernel<11><<<grid, block, 0, st>>>(a); break;
+    }
+    RKB_LAUNCHED("split_rows_fused_kernel");
     return RKB_OK;
 }
 

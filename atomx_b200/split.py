@@ -55,6 +55,36 @@ def factors_for_grid(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict
     return out
 
 
+FUSED_PASSES_MAX = 32  # passes of 32 // ng cells kept in registers by the fused row kernel
+FUSED_Z_MAX = 64
+
+
+def fused_fits(nv: int, ng: int, max_z: int) -> bool:
+    """Whether the register-resident row kernel takes this grid."""
+    return 5 <= ng <= 11 and -(-(nv - 1) // (32 // ng)) <= FUSED_PASSES_MAX and max_z <= FUSED_Z_MAX
+
+
+def fused_body_width(nv: int, ng: int) -> int:
+    """Residue positions spanned by the body in the fused layout (multiple of 128)."""
+    passes = -(-(nv - 1) // (32 // ng))
+    return 128 * (-(-passes // 4))
+
+
+def fused_body_positions(nv: int, ng: int) -> np.ndarray:
+    """Position of body column (m-1)*ng + node in the fused layout.
+
+    The kernel takes cells from the last one down, 32 // ng cells per pass,
+    lane = (cell offset within the pass) * ng + node; pass p of lane l is
+    stored at 128*(p//4) + 4*l + p%4.
+    """
+    cpp = 32 // ng
+    m = np.arange(1, nv)
+    p, sub = np.divmod(nv - 1 - m, cpp)
+    lane = sub[:, None] * ng + np.arange(ng)[None, :]
+    pos = 128 * (p[:, None] // 4) + 4 * lane + (p[:, None] % 4)
+    return pos.reshape(-1)
+
+
 def _round_up(x: int, m: int) -> int:
     return (x + m - 1) // m * m
 
@@ -65,7 +95,7 @@ class SplitEngine:
     KCHUNK = 128
 
     def __init__(self, dev: IonDevice, bits: int = DEFAULT_BITS, tau: float = 1e-3, n_mod: int | None = None,
-                 corr_floor: float | None = None):
+                 corr_floor: float | None = None, fused: bool | None = None):
         _native.require_device()
         self.dev = dev
         plan = dev.plan
@@ -85,7 +115,21 @@ class SplitEngine:
         self.koff = torch.as_tensor(koff, device=d)
         self.kbody = (nv - 1) * ng
         self.nz = {k: int(self.factors[k]["zcell"].shape[0]) for k in plan.ks}
-        self.kdim = {k: _round_up(self.kbody + self.nz[k], self.KCHUNK) for k in plan.ks}
+        max_z = max(self.nz.values())
+        fits = fused_fits(nv, ng, max_z)
+        if fused and not fits:
+            raise ValueError(f"the fused row kernel does not fit this grid (nv={nv}, ng={ng}, Z columns {max_z})")
+        #: rows in one register-resident kernel (permuted residue columns) or
+        #: in two kernels through an FP64 workspace (columns in natural order);
+        #: by default the fused kernel unless its layout adds more than 5 % to
+        #: the GEMM work (sum over k of n_k^2 * kdim_k)
+        def gemm_work(body):
+            return sum(plan.n_of_k(k) ** 2 * _round_up(body + self.nz[k], self.KCHUNK) for k in plan.ks)
+        cheap = fits and gemm_work(fused_body_width(nv, ng)) <= 1.05 * gemm_work(self.kbody)
+        self.fused = cheap if fused is None else bool(fused)
+        self.max_z = max_z
+        self.body_w = fused_body_width(nv, ng) if self.fused else self.kbody
+        self.kdim = {k: _round_up(self.body_w + self.nz[k], self.KCHUNK) for k in plan.ks}
         self.kpad = max(self.kdim.values())
         self.n_mod = int(n_mod) if n_mod is not None else moduli_needed(self.bits, self.kpad)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
@@ -101,8 +145,8 @@ class SplitEngine:
         self.left = torch.empty((nrows, self.cwp), dtype=torch.float64, device=d)
         self.right = torch.empty_like(self.left)
         self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
-        # scratch: the FP64 rows [X | Z] before they are rounded to residues
-        self.xwork = torch.empty((nrows, self.kpad), dtype=torch.float64, device=d)
+        # scratch of the two-kernel path: the FP64 rows [X | Z] before rounding
+        self.xwork = None if self.fused else torch.empty((nrows, self.kpad), dtype=torch.float64, device=d)
         zc = np.zeros(kmax + 1, dtype=np.int32)
         for k in plan.ks:
             zc[k] = self.nz[k]
@@ -129,12 +173,33 @@ class SplitEngine:
                        np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_lo)),
                        np.ctypeslib.as_ctypes(np.ascontiguousarray(np.concatenate([self.pair_inv, [1]]).astype(np.int32))))
 
-    launches_per_step = 3
     dominant_kernel = "split::crt_syrk_kernel"
+
+    @property
+    def launches_per_step(self) -> int:
+        return 2 if self.fused else 3
+
+    def column_positions(self, k: int) -> np.ndarray:
+        """Residue position of every column of the row [X | Z] of multipole k."""
+        nv, ng = self.dev.nv, self.dev.ng
+        if not self.fused:
+            return np.arange(self.kbody + self.nz[k])
+        return np.concatenate([fused_body_positions(nv, ng), self.body_w + np.arange(self.nz[k])])
 
     def rows(self, stream=None) -> None:
         L = _native.load()
         dev, plan = self.dev, self.dev.plan
+        if self.fused:
+            _native.check(L.rkb_split_rows_fused(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                                 dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                                 dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(),
+                                                 self.koff.data_ptr(), self.max_z, self.bits, self.n_mod,
+                                                 self._mod_c[0], self.resA.data_ptr(), _native.ptr(self.resB),
+                                                 self.kpad, 0, self.rows_alloc, self.rowscale.data_ptr(),
+                                                 self.left.data_ptr(), self.right.data_ptr(), self.cbound.data_ptr(),
+                                                 self.cwp, _native.stream_handle(stream)),
+                          "rkb_split_rows_fused")
+            return
         _native.check(L.rkb_split_rows(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
                                        dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
                                        dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(),
@@ -173,7 +238,7 @@ class SplitEngine:
             _native.check(st, "crt_syrk_kernel")
 
     def info(self) -> dict:
-        return {"bits": self.bits, "n_mod": self.n_mod, "moduli": [int(m) for m in self.moduli],
+        return {"bits": self.bits, "n_mod": self.n_mod, "moduli": [int(m) for m in self.moduli], "fused": self.fused,
                 "kpad": self.kpad, "z_columns": {int(k): v for k, v in self.nz.items()},
                 "tasks": self.n_tasks}
 

@@ -160,6 +160,29 @@ int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_ld, const lo
                    double *d_right, double *d_cbound, int cwp, double *d_xwork,
                    const int *d_zcount, void *stream);
 
+/* rkb_split_rows_fused: the rkb_split_rows computation in one kernel that
+ * keeps each row in registers (no FP64 workspace), for grids whose body fits:
+ * 5 <= ng <= 11, ceil((nv-1)/floor(32/ng)) <= 32 passes, at most max_z <= 64
+ * Z columns per multipole (the largest d_zcount).  Residue columns are stored
+ * in a fixed permutation shared by every row (the GEMMs are unchanged by it):
+ * with cpp = floor(32/ng), body column (m-1)*ng + node of cell m >= 1 is held
+ * in pass p = (nv-1-m) / cpp by lane l = ((nv-1-m) % cpp)*ng + node and goes
+ * to position 128*(p/4) + 4*l + (p%4); positions of lanes without a cell hold
+ * 0; Z column e goes to position rkb_split_fused_body_width(nv, ng) + e.
+ * Positions from there + nZ up to kpad are not written (keep them zero).
+ * kpad >= body width + max_z.  Scales, core vectors and bounds as in
+ * rkb_split_rows. */
+int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                         const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                         int nv, int ng, const double *d_ktab, const long *d_koff, int max_z, int bits,
+                         int n_mod, const int *moduli, signed char *d_resA, signed char *d_resB,
+                         long kpad, long row_base, long nrows_total, double *d_rowscale,
+                         double *d_left, double *d_right, double *d_cbound, int cwp, void *stream);
+
+/* Residue positions spanned by the body in rkb_split_rows_fused's layout (a
+ * multiple of 128), or -1 for an invalid grid.  Host-only, no device work. */
+long rkb_split_fused_body_width(int nv, int ng);
+
 int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, long kpad,
                        long nrows_total, int n_mod, const int *moduli, const int *pair_inv,
                        const double *f_hi,

@@ -42,9 +42,11 @@ def _engine(name, **opts):
     return ion, Pg, Qg, dev, SplitEngine(dev, **opts)
 
 
-@pytest.mark.parametrize("name", ["neon_small", "ytterbium_scaleup"])
-def test_rows_kernel_matches_cpu_transform(name):
-    ion, Pg, Qg, dev, eng = _engine(name)
+@pytest.mark.parametrize("name,fused", [("neon_small", False), ("neon_small", True),
+                                        ("ytterbium_scaleup", False), ("ytterbium_scaleup", True)])
+def test_rows_kernel_matches_cpu_transform(name, fused):
+    ion, Pg, Qg, dev, eng = _engine(name, fused=fused)
+    assert eng.fused == fused
     eng.rows()
     torch.cuda.synchronize()
     plan = dev.plan
@@ -66,20 +68,25 @@ def test_rows_kernel_matches_cpu_transform(name):
         g = rho * bd["grw"].reshape(1, -1)
         X, Z, lf, rt = transform_rows(g, F, nv, ng)
         ref = np.concatenate([X, Z], axis=1)
-        width = ref.shape[1]
-        xq = crt_exact([resA[i][rows, :width] for i in range(eng.n_mod)], eng.moduli)
+        pos = eng.column_positions(k)
+        assert pos.shape[0] == ref.shape[1]
+        xq = crt_exact([resA[i][rows][:, pos] for i in range(eng.n_mod)], eng.moduli)
         got = xq * rs[rows][:, None]
         assert np.all(np.abs(got - ref) <= (0.5 + 1e-6) * rs[rows][:, None] + 1e-15 * np.abs(ref)), k
-        assert np.all(resA[:, rows, width:] == 0)
+        unused = np.setdiff1d(np.arange(eng.kpad), pos)
+        assert np.all(resA[:, rows][:, :, unused] == 0)
         lsc = np.abs(lf).max(axis=1, keepdims=True) + 1e-300
         assert np.all(np.abs(left[rows] - lf) <= 1e-13 * lsc), k
         sc = np.abs(rt).max(axis=1, keepdims=True) + 1e-300
         assert np.all(np.abs(right[rows] - rt) <= 1e-12 * sc), k
-        if eng.resB is not None and Z.shape[1]:
+        if eng.resB is not None:
             resB = eng.resB.cpu().numpy().astype(np.int64)
-            xb = crt_exact([resB[i][rows, X.shape[1]:width] for i in range(eng.n_mod)], eng.moduli)
-            xa = crt_exact([resA[i][rows, X.shape[1]:width] for i in range(eng.n_mod)], eng.moduli)
-            np.testing.assert_array_equal(xb, -xa)
+            zpos, bpos = pos[X.shape[1]:], pos[:X.shape[1]]
+            np.testing.assert_array_equal(resB[:, rows][:, :, bpos], resA[:, rows][:, :, bpos])
+            if Z.shape[1]:
+                xb = crt_exact([resB[i][rows][:, zpos] for i in range(eng.n_mod)], eng.moduli)
+                xa = crt_exact([resA[i][rows][:, zpos] for i in range(eng.n_mod)], eng.moduli)
+                np.testing.assert_array_equal(xb, -xa)
 
 
 def _tile_check(eng, k, ti, tj):
@@ -153,12 +160,14 @@ def _schwarz_err(T, ref_vals, ii, jj):
     return np.abs(T[ii, jj] - ref_vals) / np.sqrt(d[ii] * d[jj])
 
 
-def test_split_table_neon_every_entry():
+@pytest.mark.parametrize("fused", [False, True])
+def test_split_table_neon_every_entry(fused):
     from atomx_b200 import workloads as W
     from atomx_b200.tables import slater_rk_tables
     g = np.load(os.path.join(GOLDEN, "neon_small.npz"))
     ion = W.build_ion(W.neon_small())
-    tab = slater_rk_tables(ion, precision="split")
+    tab = slater_rk_tables(ion, precision="split", fused=fused)
+    assert tab.info["fused"] == fused
     worst = 0.0
     for k in tab.ks:
         T = tab.table(k).cpu().numpy()
