@@ -783,11 +783,20 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             const bool need_corr = !(r1 * c2 <= p.corr_floor);
             constexpr int FC = 8;  // columns per final-phase chunk
+            // The final phase runs once per tile: a rolled loop keeps its code
+            // small enough to stay in the instruction cache beside the
+            // per-modulus code, so the register-resident last group is first
+            // copied to a (cached) local array that the loop can index.
+            uint32_t pk_l[EPI_COLS];
 #pragma unroll
+            for (int c = 0; c < EPI_COLS; ++c) pk_l[c] = pk[c];
+#pragma unroll 1
             for (int c = 0; c < EPI_COLS / FC; ++c) {
-                uint32_t w0[FC], w1[FC];
+                uint32_t w0[FC], w1[FC], w2[FC];
                 if (PARKED >= 1) tmem_ld8(tmem + lane_off + 256u + col0 + (uint32_t)(c * FC), w0);
                 if (PARKED >= 2) tmem_ld8(tmem + lane_off + 384u + col0 + (uint32_t)(c * FC), w1);
+#pragma unroll
+                for (int j = 0; j < FC; ++j) w2[j] = pk_l[c * FC + j];
                 tmem_wait_ld();
                 double xs[FC];
 #pragma unroll
@@ -797,7 +806,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     for (int dg = 0; dg < NDIG; ++dg) {
                         const int md = 2 * dg;              // first modulus of the digit
                         const int grp = md >> 2;
-                        const uint32_t word = grp == LASTG ? pk[c * FC + j] : (grp == 0 ? w0[j] : w1[j]);
+                        const uint32_t word = grp == LASTG ? w2[j] : (grp == 0 ? w0[j] : w1[j]);
                         const uint32_t dv = (word >> (16 * ((md >> 1) & 1))) & 0xffffu;
                         // exact int -> double: (2^52 + dv) - 2^52
                         const double r = __hiloint2double(0x43300000, (int)dv) - 4503599627370496.0;
