@@ -95,7 +95,7 @@ class SplitEngine:
     KCHUNK = 128
 
     def __init__(self, dev: IonDevice, bits: int = DEFAULT_BITS, tau: float = 1e-3, n_mod: int | None = None,
-                 corr_floor: float | None = None, fused: bool | None = None):
+                 corr_floor: float | None = None, fused: bool | None = None, materialize: bool = True):
         _native.require_device()
         self.dev = dev
         plan = dev.plan
@@ -166,8 +166,13 @@ class SplitEngine:
         tasks = tile_tasks(sizes)
         self.n_tasks = int(tasks.shape[0])
         self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
+        # task range of each group (tasks are grouped by multipole) for streaming
+        bounds = np.searchsorted(tasks[:, 0], np.arange(len(sizes) + 1))
+        self.task_range = [(int(bounds[i]), int(bounds[i + 1])) for i in range(len(sizes))]
+        self.grp_out_zero = torch.zeros(len(sizes), dtype=torch.int64, device=d)
         self.status = torch.zeros(1, dtype=torch.int32, device=d)
-        self.out = torch.empty(self.total, dtype=torch.float64, device=d)
+        #: the whole table (None when the engine only streams multipole tables)
+        self.out = torch.empty(self.total, dtype=torch.float64, device=d) if materialize else None
         self._mod_c = (np.ctypeslib.as_ctypes(np.ascontiguousarray(self.moduli, dtype=np.int32)),
                        np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_hi)),
                        np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_lo)),
@@ -211,18 +216,41 @@ class SplitEngine:
                       "rkb_split_rows")
 
     def contract(self, stream=None) -> None:
+        if self.out is None:
+            raise ValueError("this engine streams its tables (materialize=False); use stream_tables()")
+        self._contract(self.grp_out, 0, self.n_tasks, self.out, stream)
+
+    def _contract(self, grp_out, t0, t1, out, stream) -> None:
         L = _native.load()
-        plan = self.dev.plan
         _native.check(L.rkb_split_contract(self.resA.data_ptr(), _native.ptr(self.resB), self.kpad, self.rows_alloc,
                                            self.n_mod, self._mod_c[0], self._mod_c[3], self._mod_c[1], self._mod_c[2],
                                            self.M,
                                            self.rowscale.data_ptr(), self.left.data_ptr(), self.right.data_ptr(),
                                            self.cbound.data_ptr(), self.corr_floor, self.cw, self.cwp,
                                            self.grp_row0.data_ptr(), self.grp_n.data_ptr(),
-                                           self.grp_kdim.data_ptr(), self.grp_out.data_ptr(),
-                                           self.tasks.data_ptr(), self.n_tasks, self.out.data_ptr(),
+                                           self.grp_kdim.data_ptr(), grp_out.data_ptr(),
+                                           self.tasks.data_ptr() + 12 * t0, t1 - t0, out.data_ptr(),
                                            self.status.data_ptr(), _native.stream_handle(stream)),
                       "rkb_split_contract")
+
+    def stream_tables(self, sink, stream=None) -> None:
+        """Compute the rows once, then each multipole's table into one of two
+        rotating device buffers and hand it to ``sink(k, table, blocks, stream)``
+        (see ``tables.stream_tables``); the whole table is never held."""
+        s = stream if stream is not None else torch.cuda.current_stream()
+        plan = self.dev.plan
+        self.rows(s)
+        nmax = max(plan.n_of_k(k) for k in plan.ks)
+        bufs = [torch.empty(nmax * nmax, dtype=torch.float64, device=self.resA.device) for _ in range(2)]
+        #: device bytes the engine holds while streaming (buffers included)
+        self.held_bytes = self.device_bytes() + sum(b.numel() * 8 for b in bufs)
+        for gi, k in enumerate(plan.ks):
+            nk = plan.n_of_k(k)
+            t0, t1 = self.task_range[gi]
+            buf = bufs[gi % 2][:nk * nk]
+            self._contract(self.grp_out_zero, t0, t1, buf, s)
+            sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
+        self.check_status()
 
     def run(self, stream=None, upload: bool = True, check: bool = True) -> torch.Tensor:
         self.rows(stream)
@@ -230,6 +258,12 @@ class SplitEngine:
         if check:
             self.check_status()
         return self.out
+
+    def device_bytes(self) -> int:
+        """Bytes of the engine's own device buffers (not the ion's inputs)."""
+        ts = [self.ktab, self.koff, self.resA, self.resB, self.rowscale, self.left, self.right, self.cbound,
+              self.xwork, self.zcount, self.tasks, self.out]
+        return int(sum(t.numel() * t.element_size() for t in ts if t is not None))
 
     def check_status(self) -> None:
         st = int(self.status.item())
@@ -240,6 +274,7 @@ class SplitEngine:
     def info(self) -> dict:
         return {"bits": self.bits, "n_mod": self.n_mod, "moduli": [int(m) for m in self.moduli], "fused": self.fused,
                 "kpad": self.kpad, "z_columns": {int(k): v for k, v in self.nz.items()},
+                "device_bytes": self.device_bytes(),
                 "tasks": self.n_tasks}
 
     def roofline(self, stream=None, flush=None, reps: int = 3) -> dict:

@@ -27,8 +27,8 @@ from .device import as_device, resident
 from .plan import TablePlan, make_plan
 from .yk import yk_partial_matrices
 
-__all__ = ["IonDevice", "RkTables", "upload_ion", "upload_values", "slater_rk_tables",
-           "slater_rk_tables_from_values", "tables_for", "tile_tasks", "TILE"]
+__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "upload_ion", "upload_values", "slater_rk_tables",
+           "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE"]
 
 TILE = 128
 
@@ -172,6 +172,8 @@ class Fp64Workspace:
         tasks = tile_tasks(sizes)
         self.n_tasks = int(tasks.shape[0])
         self.tasks = torch.as_tensor(tasks.reshape(-1), device=self.g.device)
+        bounds = np.searchsorted(tasks[:, 0], np.arange(len(sizes) + 1))
+        self.task_range = [(int(bounds[i]), int(bounds[i + 1])) for i in range(len(sizes))]
 
 
 def run_fp64(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, stream=None) -> None:
@@ -189,12 +191,101 @@ def run_fp64(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, stream=None) 
                                             ws.n_tasks, out.data_ptr(), s), "rkb_table_contract_fp64")
 
 
-def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, **split_opts) -> RkTables:
-    """All R^k tables of one ion on the device (see module docstring)."""
+def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, sink=None,
+                     **split_opts):
+    """All R^k tables of one ion on the device (see module docstring).
+
+    With ``sink`` the tables are streamed instead of returned: the engine
+    computes one multipole table at a time into one of two rotating device
+    buffers and calls ``sink(k, table, blocks, stream)`` with the n_k x n_k
+    device view and the table's kappa-block row ranges [(block, start, stop)];
+    the view is valid for work the sink enqueues on ``stream`` (or finishes
+    before returning).  ``iter_blocks`` splits it into (k, kappa_ac-block,
+    kappa_bd-block) tiles; ``HostTableSink`` copies tables to pinned host
+    memory.  Returns an ``RkStream`` summary in that case.
+    """
     if precision not in ("fp64", "split"):
         raise ValueError(f"unknown precision {precision!r}; choose 'fp64' or 'split'")
     dev = upload_ion(ion, k_max=k_max, stream=stream)
+    if sink is not None:
+        return stream_tables(dev, sink, precision=precision, stream=stream, **split_opts)
     return tables_for(dev, precision=precision, stream=stream, **split_opts)
+
+
+@dataclass
+class RkStream:
+    """Summary of a streamed table run (the values went to the sink)."""
+    plan: TablePlan
+    ks: list
+    precision: str
+    device_bytes: int             # engine buffers held while streaming
+    info: dict = field(default_factory=dict)
+
+
+def iter_blocks(table: torch.Tensor, blocks):
+    """(kappa_ac-block, kappa_bd-block, tile view) over one multipole table."""
+    for b1, s1, e1 in blocks:
+        for b2, s2, e2 in blocks:
+            yield b1, b2, table[s1:e1, s2:e2]
+
+
+class HostTableSink:
+    """Sink that copies each multipole table to pinned host memory.
+
+    ``tables[k]`` is valid after ``wait()`` (or ``wait(k)``).
+    """
+
+    def __init__(self):
+        self.tables, self._events = {}, {}
+
+    def __call__(self, k, table, blocks, stream):
+        host = torch.empty(table.shape, dtype=table.dtype, pin_memory=True)
+        with torch.cuda.stream(stream):
+            host.copy_(table, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        self.tables[k], self._events[k] = host, ev
+
+    def wait(self, k=None):
+        for kk in ([k] if k is not None else list(self._events)):
+            self._events[kk].synchronize()
+        return self.tables if k is None else self.tables[k]
+
+
+def stream_tables(dev: IonDevice, sink, precision: str = "fp64", stream=None, **split_opts) -> RkStream:
+    """Stream every multipole table of ``dev`` to ``sink`` (see ``slater_rk_tables``)."""
+    s = stream if stream is not None else torch.cuda.current_stream()
+    plan = dev.plan
+    if precision == "split":
+        from .split import SplitEngine
+        eng = SplitEngine(dev, materialize=False, **split_opts)
+        eng.stream_tables(sink, stream=s)
+        info = eng.info()
+        held = eng.held_bytes
+    else:
+        L = _native.load()
+        ws = Fp64Workspace(dev)
+        h = _native.stream_handle(s)
+        _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                            dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                            dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
+                                            dev.mi.data_ptr(), ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, h),
+                      "rkb_table_rows_fp64")
+        nmax = max(plan.n_of_k(k) for k in plan.ks)
+        bufs = [torch.empty(nmax * nmax, dtype=torch.float64, device=dev.Pv.device) for _ in range(2)]
+        zero = torch.zeros(len(plan.ks), dtype=torch.int64, device=dev.Pv.device)
+        held = (ws.g.numel() + ws.y.numel() + 2 * nmax * nmax) * 8
+        for gi, k in enumerate(plan.ks):
+            nk = plan.n_of_k(k)
+            t0, t1 = ws.task_range[gi]
+            buf = bufs[gi % 2][:nk * nk]
+            _native.check(L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld,
+                                                    ws.row0.data_ptr(), ws.nk.data_ptr(), zero.data_ptr(),
+                                                    ws.tasks.data_ptr() + 12 * t0, t1 - t0, buf.data_ptr(), h),
+                          "rkb_table_contract_fp64")
+            sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
+        info = {}
+    return RkStream(plan=plan, ks=plan.ks, precision=precision, device_bytes=int(held), info=info)
 
 
 def slater_rk_tables_from_values(Pv, Qv, kappa, gr, grw, k_max: int, precision: str = "fp64", stream=None,
