@@ -31,6 +31,7 @@ _SIGNATURES = {
     "rkb_slater_direct": [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp],
     "rkb_table_rows_fp64": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _l, _vp],
     "rkb_table_contract_fp64": [_vp, _vp, _l, _l, _vp, _vp, _vp, _vp, _l, _vp, _vp],
+    "rkb_table_contract_fp64_groups": [_vp, _vp, _l, _l, _vp, _vp, _vp, _vp, _vp, _l, _vp, _vp],
     "rkb_split_rows": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _l, _l,
                        _l, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp],
     "rkb_split_rows_noalloc": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _i, _i, _vp, _vp, _vp, _l,

@@ -1,0 +1,271 @@
+"""Many ions' R^k tables in one persistent launch, replayed as a CUDA graph.
+
+A batch concatenates the (pair, k) rows of every ion into one row space.
+One contraction launch then covers the upper tiles of every (ion, k) table:
+persistent CTAs walk a single task list, and each task carries its group's
+row offset, size and contraction length. Ions of different grids (N, n_gauss)
+and table sizes therefore share the launch. The per-ion row kernels (grids
+differ per ion) and the contraction are captured once into a CUDA graph and
+replayed.
+
+* ``SplitBatch``: the split engine. Every ion's rows are written into one
+  pair of int8 residue matrices through ``split.IonRows``, and one
+  ``crt_syrk_kernel`` runs over all (ion, k) groups.
+* ``Fp64Batch``: the plain engine. Every ion's g and Y^k rows go into one
+  (rows, ld) pair, and one ``fp64tab::contract_kernel`` runs with a
+  contraction length per group.
+
+The task order matters for balance: tasks cost in proportion to their
+group's contraction length, and persistent CTAs take tasks round-robin.
+``order="lpt"`` sorts tasks by decreasing cost (longest first); ``"group"``
+keeps the table order. ``atomx_b200.autotune`` picks the order, the split
+width (bits, and so the number of moduli) and the row-kernel layout by
+timing them on the batch under the error gate.
+
+This has no single atomx counterpart. atomx computes each table with
+per-integral ``slater_rk_poisson`` calls (numerics/bspline/slater.py:118) or
+``compute_slater_rk_table`` (numerics/bspline/convol.py:1988) per ion.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native
+from .split import IonRows, _round_up, choose_width
+from .split_plan import crt_constants
+from .tables import IonDevice, RkTables, TILE
+
+__all__ = ["SplitBatch", "Fp64Batch", "batch_tasks"]
+
+
+def batch_tasks(sizes, costs, order: str = "lpt") -> np.ndarray:
+    """Upper-triangle tile tasks (group, ti, tj) of all groups, ordered.
+
+    ``costs[g]`` is the relative cost of one tile of group g (its
+    contraction length). "lpt" puts the most expensive tiles first (persistent
+    CTAs then finish close together); "group" keeps groups in order.
+    """
+    out = []
+    for g, n in enumerate(sizes):
+        nt = (int(n) + TILE - 1) // TILE
+        for ti in range(nt):
+            for tj in range(ti, nt):
+                out.append((g, ti, tj))
+    tasks = np.asarray(out, dtype=np.int32).reshape(-1, 3)
+    if order == "lpt" and tasks.shape[0]:
+        c = np.asarray(costs, dtype=np.float64)[tasks[:, 0]]
+        tasks = tasks[np.argsort(-c, kind="stable")]
+    elif order != "group":
+        raise ValueError(f"unknown task order {order!r}")
+    return tasks
+
+
+class _Graphable:
+    """Shared CUDA-graph capture of ``step()``."""
+
+    graph = None
+
+    def capture(self, stream=None):
+        """Record ``step()`` once into a CUDA graph (after one eager warm-up,
+        which also performs every one-time attribute set-up)."""
+        s = stream if stream is not None else torch.cuda.Stream()
+        self.step(s)
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            self.step(s)
+        self.graph = g
+        return g
+
+    def replay(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+
+class SplitBatch(_Graphable):
+    """Split-precision tables of many ions with one contraction launch."""
+
+    dominant_kernel = "split::crt_syrk_kernel"
+
+    def __init__(self, devs: list[IonDevice], bits: int | None = None, tau: float = 1e-3, fused=None,
+                 corr_floor: float | None = None, order: str = "lpt", n_mod: int | None = None):
+        _native.require_device()
+        if not devs:
+            raise ValueError("empty batch")
+        self.devs, self.order = list(devs), order
+        self.ions = [IonRows(d, tau=tau, fused=fused) for d in self.devs]
+        d = self.devs[0].Pv.device
+        self.kpad = max(r.kmax_dim for r in self.ions)
+        self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
+        self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
+        self.cw = max(dv.ng for dv in self.devs)
+        self.cwp = _round_up(self.cw, 2)
+        counts = [dv.plan.n_rows for dv in self.devs]
+        self.row_base = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        nrows = int(self.row_base[-1])
+        self.rows_alloc = _round_up(max(nrows, 1), TILE)
+        self.resA = torch.zeros((self.n_mod, self.rows_alloc, self.kpad), dtype=torch.int8, device=d)
+        self.resB = torch.zeros_like(self.resA) if any(r.has_z for r in self.ions) else None
+        self.rowscale = torch.empty(nrows, dtype=torch.float64, device=d)
+        self.left = torch.zeros((nrows, self.cwp), dtype=torch.float64, device=d)
+        self.right = torch.zeros_like(self.left)
+        self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
+        two = [dv.plan.n_rows for dv, r in zip(self.devs, self.ions) if not r.fused]
+        self.xwork = torch.empty((max(two), self.kpad), dtype=torch.float64, device=d) if two else None
+        self.corr_floor = 2.0 ** -(self.bits + 10) if corr_floor is None else float(corr_floor)
+        # groups: (ion, k)
+        g_row0, g_n, g_kdim, self.group_of = [], [], [], []
+        for i, (dv, r) in enumerate(zip(self.devs, self.ions)):
+            for k in dv.plan.ks:
+                g_row0.append(int(self.row_base[i]) + dv.plan.k_row_offset[k])
+                g_n.append(dv.plan.n_of_k(k))
+                g_kdim.append(r.kdim[k])
+                self.group_of.append((i, k))
+        offs = np.concatenate([[0], np.cumsum(np.asarray(g_n, dtype=np.int64) ** 2)])
+        self.offsets = {gk: int(offs[j]) for j, gk in enumerate(self.group_of)}
+        self.total = int(offs[-1])
+        self.grp_row0 = torch.as_tensor(g_row0, dtype=torch.int64, device=d)
+        self.grp_n = torch.as_tensor(g_n, dtype=torch.int64, device=d)
+        self.grp_kdim = torch.as_tensor(g_kdim, dtype=torch.int64, device=d)
+        self.grp_out = torch.as_tensor(offs[:-1], dtype=torch.int64, device=d)
+        tasks = batch_tasks(g_n, g_kdim, order)
+        self.n_tasks = int(tasks.shape[0])
+        self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
+        self.status = torch.zeros(1, dtype=torch.int32, device=d)
+        self.out = torch.empty(self.total, dtype=torch.float64, device=d)
+        self._c = (np.ctypeslib.as_ctypes(np.ascontiguousarray(self.moduli, dtype=np.int32)),
+                   np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_hi)),
+                   np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_lo)),
+                   np.ctypeslib.as_ctypes(np.ascontiguousarray(np.concatenate([self.pair_inv, [1]]).astype(np.int32))))
+
+    @property
+    def launches_per_step(self) -> int:
+        return sum(1 if r.fused else 2 for r in self.ions) + 1
+
+    @property
+    def ordered_entries(self) -> int:
+        return sum(dv.plan.ordered_entries for dv in self.devs)
+
+    def rows(self, stream=None) -> None:
+        for i, r in enumerate(self.ions):
+            r.launch(self.bits, self.n_mod, self._c[0], self.resA, self.resB, self.kpad, int(self.row_base[i]),
+                     self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp, self.xwork,
+                     stream)
+
+    def contract(self, stream=None) -> None:
+        L = _native.load()
+        _native.check(L.rkb_split_contract(self.resA.data_ptr(), _native.ptr(self.resB), self.kpad, self.rows_alloc,
+                                           self.n_mod, self._c[0], self._c[3], self._c[1], self._c[2], self.M,
+                                           self.rowscale.data_ptr(), self.left.data_ptr(), self.right.data_ptr(),
+                                           self.cbound.data_ptr(), self.corr_floor, self.cw, self.cwp,
+                                           self.grp_row0.data_ptr(), self.grp_n.data_ptr(),
+                                           self.grp_kdim.data_ptr(), self.grp_out.data_ptr(), self.tasks.data_ptr(),
+                                           self.n_tasks, self.out.data_ptr(), self.status.data_ptr(),
+                                           _native.stream_handle(stream)),
+                      "rkb_split_contract")
+
+    def step(self, stream=None) -> None:
+        """Enqueue every row launch and the one contraction (no host sync)."""
+        self.rows(stream)
+        self.contract(stream)
+
+    def check_status(self) -> None:
+        st = int(self.status.item())
+        if st:
+            self.status.zero_()
+            _native.check(st, "crt_syrk_kernel")
+
+    def table(self, ion: int, k: int) -> torch.Tensor:
+        nk = self.devs[ion].plan.n_of_k(k)
+        o = self.offsets[(ion, k)]
+        return self.out[o:o + nk * nk].view(nk, nk)
+
+    def tables(self, ion: int) -> RkTables:
+        plan = self.devs[ion].plan
+        o0 = self.offsets[(ion, plan.ks[0])]
+        n = sum(plan.n_of_k(k) ** 2 for k in plan.ks)
+        return RkTables(plan=plan, ks=plan.ks, values=self.out[o0:o0 + n],
+                        offsets={k: self.offsets[(ion, k)] - o0 for k in plan.ks}, precision="split",
+                        info={"bits": self.bits, "n_mod": self.n_mod, "fused": self.ions[ion].fused})
+
+    def info(self) -> dict:
+        return {"ions": len(self.devs), "bits": self.bits, "n_mod": self.n_mod, "kpad": self.kpad,
+                "order": self.order, "tasks": self.n_tasks, "rows": int(self.row_base[-1]),
+                "fused_ions": int(sum(r.fused for r in self.ions)), "entries": self.ordered_entries}
+
+
+class Fp64Batch(_Graphable):
+    """Plain FP64 tables of many ions with one contraction launch."""
+
+    dominant_kernel = "fp64tab::contract_kernel"
+
+    def __init__(self, devs: list[IonDevice], order: str = "lpt"):
+        _native.require_device()
+        if not devs:
+            raise ValueError("empty batch")
+        self.devs, self.order = list(devs), order
+        d = self.devs[0].Pv.device
+        self.ld = _round_up(max(dv.n for dv in self.devs), 32)
+        counts = [dv.plan.n_rows for dv in self.devs]
+        self.row_base = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        nrows = int(self.row_base[-1])
+        self.g = torch.empty((nrows, self.ld), dtype=torch.float64, device=d)
+        self.y = torch.empty_like(self.g)
+        g_row0, g_n, g_kdim, self.group_of = [], [], [], []
+        for i, dv in enumerate(self.devs):
+            for k in dv.plan.ks:
+                g_row0.append(int(self.row_base[i]) + dv.plan.k_row_offset[k])
+                g_n.append(dv.plan.n_of_k(k))
+                g_kdim.append(_round_up(dv.n, 16))
+                self.group_of.append((i, k))
+        self.max_kdim = max(g_kdim)
+        offs = np.concatenate([[0], np.cumsum(np.asarray(g_n, dtype=np.int64) ** 2)])
+        self.offsets = {gk: int(offs[j]) for j, gk in enumerate(self.group_of)}
+        self.total = int(offs[-1])
+        self.grp_row0 = torch.as_tensor(g_row0, dtype=torch.int64, device=d)
+        self.grp_n = torch.as_tensor(g_n, dtype=torch.int64, device=d)
+        self.grp_kdim = torch.as_tensor(g_kdim, dtype=torch.int64, device=d)
+        self.grp_out = torch.as_tensor(offs[:-1], dtype=torch.int64, device=d)
+        tasks = batch_tasks(g_n, g_kdim, order)
+        self.n_tasks = int(tasks.shape[0])
+        self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
+        self.out = torch.empty(self.total, dtype=torch.float64, device=d)
+
+    @property
+    def launches_per_step(self) -> int:
+        return len(self.devs) + 1
+
+    @property
+    def ordered_entries(self) -> int:
+        return sum(dv.plan.ordered_entries for dv in self.devs)
+
+    def step(self, stream=None) -> None:
+        L = _native.load()
+        h = _native.stream_handle(stream)
+        for i, dv in enumerate(self.devs):
+            off = int(self.row_base[i]) * self.ld * 8
+            _native.check(L.rkb_table_rows_fp64(dv.Pv.data_ptr(), dv.Qv.data_ptr(), dv.n, dv.pairs.data_ptr(),
+                                                dv.row_pair.data_ptr(), dv.row_k.data_ptr(), dv.plan.n_rows,
+                                                dv.r.data_ptr(), dv.w.data_ptr(), dv.nv, dv.ng, dv.mo.data_ptr(),
+                                                dv.mi.data_ptr(), self.g.data_ptr() + off, self.y.data_ptr() + off,
+                                                self.ld, h),
+                          "rkb_table_rows_fp64")
+        _native.check(L.rkb_table_contract_fp64_groups(self.g.data_ptr(), self.y.data_ptr(), self.ld, self.max_kdim,
+                                                       self.grp_kdim.data_ptr(), self.grp_row0.data_ptr(),
+                                                       self.grp_n.data_ptr(), self.grp_out.data_ptr(),
+                                                       self.tasks.data_ptr(), self.n_tasks, self.out.data_ptr(), h),
+                      "rkb_table_contract_fp64_groups")
+
+    def check_status(self) -> None:
+        return None
+
+    def table(self, ion: int, k: int) -> torch.Tensor:
+        nk = self.devs[ion].plan.n_of_k(k)
+        o = self.offsets[(ion, k)]
+        return self.out[o:o + nk * nk].view(nk, nk)
+
+    def info(self) -> dict:
+        return {"ions": len(self.devs), "ld": self.ld, "order": self.order, "tasks": self.n_tasks,
+                "rows": int(self.row_base[-1]), "entries": self.ordered_entries}

@@ -41,6 +41,13 @@ inline long ceil_div(long a, long b) { return (a + b - 1) / b; }
 // Number of SMs on the current device (cached per device).
 int sm_count();
 
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per (kernel, device,
+// size): later launches (e.g. while a stream is being captured into a CUDA
+// graph) make no attribute call.
+cudaError_t set_smem_once(const void *func, int bytes);
+template <class F>
+inline cudaError_t set_smem(F *func, int bytes) { return set_smem_once(reinterpret_cast<const void *>(func), bytes); }
+
 // ---------------------------------------------------------------- device side
 // x^n for integer n by square-and-multiply, negative n as 1/x^|n|: the same
 // operation sequence Numba emits for float**int, so powers agree bit for bit

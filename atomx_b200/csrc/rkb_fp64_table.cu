@@ -50,18 +50,18 @@ __device__ __forceinline__ void load_tile(double *s, const double *__restrict__ 
 
 __global__ void __launch_bounds__(THREADS, 1)
 contract_kernel(const double *__restrict__ G, const double *__restrict__ Y, long ld, long kdim,
-                const long *__restrict__ grp_row0, const long *__restrict__ grp_n, const long *__restrict__ grp_out,
-                const int *__restrict__ tasks, long n_tasks, double *__restrict__ out) {
+                const long *__restrict__ grp_kdim, const long *__restrict__ grp_row0, const long *__restrict__ grp_n,
+                const long *__restrict__ grp_out, const int *__restrict__ tasks, long n_tasks,
+                double *__restrict__ out) {
     extern __shared__ double smem[];
     double *As = smem;
     double *Bs = smem + STAGES * BM * LDS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = warp >> 2, wn = warp & 3;
     const int fr = lane >> 2, fc = lane & 3;
-    const int nk = (int)(kdim / BK);
-
     for (long t = blockIdx.x; t < n_tasks; t += gridDim.x) {
         const int g = tasks[3 * t], ti = tasks[3 * t + 1], tj = tasks[3 * t + 2];
+        const int nk = (int)((grp_kdim ? grp_kdim[g] : kdim) / BK);
         const long row0 = grp_row0[g], n = grp_n[g];
         const long i0 = (long)ti * BM, j0 = (long)tj * BN;
         const double *Ag = G + row0 * ld, *Bg = Y + row0 * ld;
@@ -133,17 +133,35 @@ contract_kernel(const double *__restrict__ G, const double *__restrict__ Y, long
 
 using namespace rkb;
 
+static int launch_contract(const double *d_g, const double *d_y, long ld, long kdim, const long *d_grp_kdim,
+                           const long *d_grp_row0, const long *d_grp_n, const long *d_grp_out, const int *d_tasks,
+                           long n_tasks, double *d_out, void *stream) {
+    if (n_tasks == 0) return RKB_OK;
+    auto kern = fp64tab::contract_kernel;
+    RKB_CUDA(set_smem(kern, (int)fp64tab::SMEM));
+    long grid = n_tasks < sm_count() ? n_tasks : sm_count();
+    kern<<<(unsigned)grid, fp64tab::THREADS, fp64tab::SMEM, as_stream(stream)>>>(
+        d_g, d_y, ld, kdim, d_grp_kdim, d_grp_row0, d_grp_n, d_grp_out, d_tasks, n_tasks, d_out);
+    RKB_LAUNCHED("fp64tab::contract_kernel");
+    return RKB_OK;
+}
+
 extern "C" int rkb_table_contract_fp64(const double *d_g, const double *d_y, long ld, long kdim,
                                        const long *d_grp_row0, const long *d_grp_n, const long *d_grp_out,
                                        const int *d_tasks, long n_tasks, double *d_out, void *stream) {
     RKB_CHECK_ARG(kdim >= 0 && kdim % fp64tab::BK == 0 && ld >= kdim && ld % 2 == 0,
                   "contraction length %ld must be a multiple of %d and <= ld (%ld, even)", kdim, fp64tab::BK, ld);
-    if (n_tasks == 0) return RKB_OK;
-    auto kern = fp64tab::contract_kernel;
-    RKB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fp64tab::SMEM));
-    long grid = n_tasks < sm_count() ? n_tasks : sm_count();
-    kern<<<(unsigned)grid, fp64tab::THREADS, fp64tab::SMEM, as_stream(stream)>>>(
-        d_g, d_y, ld, kdim, d_grp_row0, d_grp_n, d_grp_out, d_tasks, n_tasks, d_out);
-    RKB_LAUNCHED("fp64tab::contract_kernel");
-    return RKB_OK;
+    return launch_contract(d_g, d_y, ld, kdim, nullptr, d_grp_row0, d_grp_n, d_grp_out, d_tasks, n_tasks, d_out,
+                           stream);
+}
+
+extern "C" int rkb_table_contract_fp64_groups(const double *d_g, const double *d_y, long ld, long max_kdim,
+                                              const long *d_grp_kdim, const long *d_grp_row0, const long *d_grp_n,
+                                              const long *d_grp_out, const int *d_tasks, long n_tasks,
+                                              double *d_out, void *stream) {
+    RKB_CHECK_ARG(d_grp_kdim != nullptr, "per-group contraction lengths are required");
+    RKB_CHECK_ARG(max_kdim >= 0 && ld >= max_kdim && ld % 2 == 0, "contraction lengths must be <= ld (%ld, even)",
+                  ld);
+    return launch_contract(d_g, d_y, ld, max_kdim, d_grp_kdim, d_grp_row0, d_grp_n, d_grp_out, d_tasks, n_tasks,
+                           d_out, stream);
 }

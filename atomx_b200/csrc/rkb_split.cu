@@ -952,15 +952,14 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
                   "residue buffers must be 16-byte aligned");
 #define RKB_SR_CASE(NGV)                                                                              \
     case NGV: {                                                                                       \
-        RKB_CUDA(cudaFuncSetAttribute(split_rows_kernel<NGV>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                      (int)smem));                                                    \
+        RKB_CUDA(set_smem(split_rows_kernel<NGV>, (int)smem));                                         \
         split_rows_kernel<NGV><<<grid, block, smem, st>>>(a);                                         \
         break;                                                                                        \
     }
     switch (ng) {
         RKB_SR_CASE(5) RKB_SR_CASE(7) RKB_SR_CASE(8) RKB_SR_CASE(9) RKB_SR_CASE(11)
         default: {
-            RKB_CUDA(cudaFuncSetAttribute(split_rows_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            RKB_CUDA(set_smem(split_rows_kernel<0>, (int)smem));
             split_rows_kernel<0><<<grid, block, smem, st>>>(a);
         }
     }
@@ -1068,8 +1067,7 @@ extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *
     cudaStream_t st = as_stream(stream);
 #define RKB_CRT_CASE(NM)                                                                                     \
     case NM: {                                                                                               \
-        RKB_CUDA(cudaFuncSetAttribute(crt_syrk_kernel<NM>, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
-                                      (int)SMEM_BYTES));                                                     \
+        RKB_CUDA(set_smem(crt_syrk_kernel<NM>, (int)SMEM_BYTES));                                            \
         crt_syrk_kernel<NM><<<(unsigned)grid, THREADS, SMEM_BYTES, st>>>(mA, mB, p);                         \
         break;                                                                                               \
     }

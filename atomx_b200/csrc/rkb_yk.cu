@@ -15,6 +15,8 @@
 // reference is the association order of the cross-cell base sums.
 #include <cstdarg>
 #include <mutex>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "rkb_common.cuh"
@@ -34,6 +36,21 @@ void set_error(const char *fmt, ...) {
 int cuda_status(cudaError_t err, const char *what) {
     set_error("CUDA error in %s: %s (%s)", what, cudaGetErrorName(err), cudaGetErrorString(err));
     return RKB_ECUDA;
+}
+
+cudaError_t set_smem_once(const void *func, int bytes) {
+    // the attribute only ever grows, so a smaller request never undoes a larger one
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int &cur = limit[std::make_pair(func, dev)];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
 }
 
 int sm_count() {
@@ -190,7 +207,7 @@ static int launch_yk(Src src, const int *d_row_k, int k_all, long nrows, const d
 #define RKB_YK_CASE(NGV)                                                                                  \
     case NGV: {                                                                                           \
         auto kern = yk_rows_kernel<NGV, Src>;                                                             \
-        RKB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
+        RKB_CUDA(set_smem(kern, (int)smem));     \
         kern<<<grid, block, smem, st>>>(src, d_row_k, k_all, nrows, d_r, d_w, nv, ng, d_mo, d_mi, d_yk,   \
                                         yk_ld, d_g);                                                      \
         break;                                                                                            \
@@ -201,7 +218,7 @@ static int launch_yk(Src src, const int *d_row_k, int k_all, long nrows, const d
         RKB_YK_CASE(16) RKB_YK_CASE(17)
         default: {
             auto kern = yk_rows_kernel<0, Src>;
-            RKB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            RKB_CUDA(set_smem(kern, (int)smem));
             kern<<<grid, block, smem, st>>>(src, d_row_k, k_all, nrows, d_r, d_w, nv, ng, d_mo, d_mi, d_yk, yk_ld,
                                             d_g);
         }

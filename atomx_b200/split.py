@@ -26,12 +26,25 @@ import numpy as np
 import torch
 
 from . import _native
-from .split_plan import crt_constants, green_factor, moduli_needed, pack_factors
+from .split_plan import bits_for_moduli, crt_constants, green_factor, moduli_needed, pack_factors
 from .tables import IonDevice, tile_tasks
 
-__all__ = ["SplitEngine", "factors_for_grid", "DEFAULT_BITS"]
+__all__ = ["SplitEngine", "IonRows", "factors_for_grid", "choose_width", "DEFAULT_BITS"]
 
+#: the split is at least this wide by default; ``bits=None`` then widens it to
+#: what the same number of CRT moduli still holds exactly (free accuracy)
 DEFAULT_BITS = 36
+
+
+def choose_width(bits, n_mod, kdim: int) -> tuple[int, int]:
+    """(bits, n_mod) for a contraction length: explicit values are kept;
+    bits=None takes the fewest moduli for DEFAULT_BITS and the widest split
+    those moduli hold."""
+    if bits is not None:
+        bits = int(bits)
+        return bits, (int(n_mod) if n_mod is not None else moduli_needed(bits, kdim))
+    n_mod = int(n_mod) if n_mod is not None else moduli_needed(DEFAULT_BITS, kdim)
+    return max(DEFAULT_BITS, bits_for_moduli(n_mod, kdim)), n_mod
 _factor_cache: dict = {}
 _factor_lock = threading.Lock()
 
@@ -89,17 +102,16 @@ def _round_up(x: int, m: int) -> int:
     return (x + m - 1) // m * m
 
 
-class SplitEngine:
-    """Device buffers and launch plan of the split engine for one ion."""
+class IonRows:
+    """Row side of the split engine for one ion: factor tables on the device,
+    the residue layout (fused register kernel or two-kernel path) and the
+    launch that writes the ion's rows into shared residue matrices."""
 
     KCHUNK = 128
 
-    def __init__(self, dev: IonDevice, bits: int = DEFAULT_BITS, tau: float = 1e-3, n_mod: int | None = None,
-                 corr_floor: float | None = None, fused: bool | None = None, materialize: bool = True):
-        _native.require_device()
+    def __init__(self, dev: IonDevice, tau: float = 1e-3, fused: bool | None = None):
         self.dev = dev
         plan = dev.plan
-        self.bits = int(bits)
         nv, ng = dev.nv, dev.ng
         r_host = dev.extra.get("r_host")
         if r_host is None:
@@ -119,19 +131,80 @@ class SplitEngine:
         fits = fused_fits(nv, ng, max_z)
         if fused and not fits:
             raise ValueError(f"the fused row kernel does not fit this grid (nv={nv}, ng={ng}, Z columns {max_z})")
-        #: rows in one register-resident kernel (permuted residue columns) or
-        #: in two kernels through an FP64 workspace (columns in natural order);
-        #: by default the fused kernel unless its layout adds more than 5 % to
-        #: the GEMM work (sum over k of n_k^2 * kdim_k)
+
+        # rows in one register-resident kernel (permuted residue columns) or in
+        # two kernels through an FP64 workspace (columns in natural order); by
+        # default the fused kernel unless its layout adds more than 5 % to the
+        # GEMM work (sum over k of n_k^2 * kdim_k)
         def gemm_work(body):
             return sum(plan.n_of_k(k) ** 2 * _round_up(body + self.nz[k], self.KCHUNK) for k in plan.ks)
+
         cheap = fits and gemm_work(fused_body_width(nv, ng)) <= 1.05 * gemm_work(self.kbody)
         self.fused = cheap if fused is None else bool(fused)
         self.max_z = max_z
         self.body_w = fused_body_width(nv, ng) if self.fused else self.kbody
         self.kdim = {k: _round_up(self.body_w + self.nz[k], self.KCHUNK) for k in plan.ks}
+        self.kmax_dim = max(self.kdim.values())
+        self.has_z = max_z > 0
+        zc = np.zeros(kmax + 1, dtype=np.int32)
+        for k in plan.ks:
+            zc[k] = self.nz[k]
+        self.zcount = torch.as_tensor(zc, device=d)
+
+    def column_positions(self, k: int) -> np.ndarray:
+        """Residue position of every column of the row [X | Z] of multipole k."""
+        nv, ng = self.dev.nv, self.dev.ng
+        if not self.fused:
+            return np.arange(self.kbody + self.nz[k])
+        return np.concatenate([fused_body_positions(nv, ng), self.body_w + np.arange(self.nz[k])])
+
+    def launch(self, bits: int, n_mod: int, moduli_c, resA, resB, kpad: int, row_base: int, nrows_total: int,
+               rowscale, left, right, cbound, cwp: int, xwork, stream) -> None:
+        """Write this ion's rows at rows [row_base, row_base + n_rows) of the
+        [modulus][row][kpad] residue matrices (resA/resB, nrows_total rows)."""
+        L = _native.load()
+        dev, plan = self.dev, self.dev.plan
+        rb = int(row_base)
+        # the row range is folded into the base pointers (every modulus slab
+        # shifts by the same row offset), so each launch sees rows from 0
+        a_ptr = resA.data_ptr() + rb * kpad
+        b_ptr = resB.data_ptr() + rb * kpad if resB is not None else 0
+        rs, lf = rowscale.data_ptr() + 8 * rb, left.data_ptr() + 8 * rb * cwp
+        rt, cb = right.data_ptr() + 8 * rb * cwp, cbound.data_ptr() + 16 * rb
+        if self.fused:
+            _native.check(L.rkb_split_rows_fused(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                                 dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                                 dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(),
+                                                 self.koff.data_ptr(), self.max_z, bits, n_mod, moduli_c, a_ptr,
+                                                 b_ptr, kpad, 0, nrows_total, rs, lf, rt, cb, cwp,
+                                                 _native.stream_handle(stream)),
+                          "rkb_split_rows_fused")
+            return
+        _native.check(L.rkb_split_rows(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                       dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                       dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(), self.koff.data_ptr(),
+                                       bits, n_mod, moduli_c, a_ptr, b_ptr, kpad, 0, nrows_total, rs, lf, rt, cb,
+                                       cwp, xwork.data_ptr(), self.zcount.data_ptr(), _native.stream_handle(stream)),
+                      "rkb_split_rows")
+
+
+class SplitEngine:
+    """Device buffers and launch plan of the split engine for one ion."""
+
+    KCHUNK = 128
+
+    def __init__(self, dev: IonDevice, bits: int | None = None, tau: float = 1e-3, n_mod: int | None = None,
+                 corr_floor: float | None = None, fused: bool | None = None, materialize: bool = True):
+        _native.require_device()
+        self.dev = dev
+        plan = dev.plan
+        nv, ng = dev.nv, dev.ng
+        self.ion_rows = R = IonRows(dev, tau=tau, fused=fused)
+        self.factors, self.ktab, self.koff, self.kbody, self.nz = R.factors, R.ktab, R.koff, R.kbody, R.nz
+        self.fused, self.max_z, self.body_w, self.kdim, self.zcount = R.fused, R.max_z, R.body_w, R.kdim, R.zcount
+        d = dev.Pv.device
         self.kpad = max(self.kdim.values())
-        self.n_mod = int(n_mod) if n_mod is not None else moduli_needed(self.bits, self.kpad)
+        self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
         self.cw = ng
         self.cwp = _round_up(self.cw, 2)
@@ -147,10 +220,6 @@ class SplitEngine:
         self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
         # scratch of the two-kernel path: the FP64 rows [X | Z] before rounding
         self.xwork = None if self.fused else torch.empty((nrows, self.kpad), dtype=torch.float64, device=d)
-        zc = np.zeros(kmax + 1, dtype=np.int32)
-        for k in plan.ks:
-            zc[k] = self.nz[k]
-        self.zcount = torch.as_tensor(zc, device=d)
         #: skip the FP64 core correction of a block when its bound is below
         #: 2^-(bits+10) of the block's scale (none of the entries can move by
         #: more than that; the split's own error is ~2^-bits of the same scale)
@@ -186,34 +255,12 @@ class SplitEngine:
 
     def column_positions(self, k: int) -> np.ndarray:
         """Residue position of every column of the row [X | Z] of multipole k."""
-        nv, ng = self.dev.nv, self.dev.ng
-        if not self.fused:
-            return np.arange(self.kbody + self.nz[k])
-        return np.concatenate([fused_body_positions(nv, ng), self.body_w + np.arange(self.nz[k])])
+        return self.ion_rows.column_positions(k)
 
     def rows(self, stream=None) -> None:
-        L = _native.load()
-        dev, plan = self.dev, self.dev.plan
-        if self.fused:
-            _native.check(L.rkb_split_rows_fused(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
-                                                 dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
-                                                 dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(),
-                                                 self.koff.data_ptr(), self.max_z, self.bits, self.n_mod,
-                                                 self._mod_c[0], self.resA.data_ptr(), _native.ptr(self.resB),
-                                                 self.kpad, 0, self.rows_alloc, self.rowscale.data_ptr(),
-                                                 self.left.data_ptr(), self.right.data_ptr(), self.cbound.data_ptr(),
-                                                 self.cwp, _native.stream_handle(stream)),
-                          "rkb_split_rows_fused")
-            return
-        _native.check(L.rkb_split_rows(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
-                                       dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
-                                       dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(),
-                                       self.koff.data_ptr(), self.bits, self.n_mod, self._mod_c[0],
-                                       self.resA.data_ptr(), _native.ptr(self.resB), self.kpad, 0, self.rows_alloc,
-                                       self.rowscale.data_ptr(), self.left.data_ptr(), self.right.data_ptr(),
-                                       self.cbound.data_ptr(), self.cwp, self.xwork.data_ptr(),
-                                       self.zcount.data_ptr(), _native.stream_handle(stream)),
-                      "rkb_split_rows")
+        self.ion_rows.launch(self.bits, self.n_mod, self._mod_c[0], self.resA, self.resB, self.kpad, 0,
+                             self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp,
+                             self.xwork, stream)
 
     def contract(self, stream=None) -> None:
         if self.out is None:

@@ -59,8 +59,8 @@ import numpy as np
 
 from .yk import yk_partial_matrices
 
-__all__ = ["MODULI", "crt_constants", "digit_moduli", "moduli_needed", "green_factor", "pack_factors",
-           "factor_table_layout"]
+__all__ = ["MODULI", "bits_for_moduli", "crt_constants", "digit_moduli", "moduli_needed", "green_factor",
+           "pack_factors", "factor_table_layout"]
 
 #: Pairwise-coprime moduli, largest first (256 = 2^8; 255 = 3*5*17; 253 = 11*23;
 #: 247 = 13*19; 217 = 7*31; the rest are primes).
@@ -77,6 +77,16 @@ def moduli_needed(bits: int, kdim: int) -> int:
         if prod > need:
             return i + 1
     raise ValueError(f"{bits}-bit splits of length {kdim} need more than {MAX_MODULI} int8 moduli")
+
+
+def bits_for_moduli(n_mod: int, kdim: int, cap: int = 40) -> int:
+    """Widest split (bits, at most ``cap``) whose products the first n_mod moduli
+    still hold exactly: the largest b with 2 * kdim * 2^(2b) + 2 < prod m_i."""
+    M = math.prod(MODULI[:n_mod])
+    b = 0
+    while b < cap and 2 * kdim * (1 << (2 * (b + 1))) + 2 < M:
+        b += 1
+    return b
 
 
 def digit_moduli(n_mod: int) -> list[int]:

@@ -115,6 +115,16 @@ int rkb_table_contract_fp64(const double *d_g, const double *d_y, long ld, long 
                             const long *d_grp_row0, const long *d_grp_n, const long *d_grp_out,
                             const int *d_tasks, long n_tasks, double *d_out, void *stream);
 
+/* As rkb_table_contract_fp64 with a contraction length per group,
+ * d_grp_kdim[g] (each a multiple of 16 and <= max_kdim <= ld): one
+ * persistent launch over the groups of many ions with different grids, whose
+ * rows share one (g, y) matrix of stride ld (atomx has no batched
+ * counterpart; each group is a table of slater_rk_poisson values). */
+int rkb_table_contract_fp64_groups(const double *d_g, const double *d_y, long ld, long max_kdim,
+                                   const long *d_grp_kdim, const long *d_grp_row0, const long *d_grp_n,
+                                   const long *d_grp_out, const int *d_tasks, long n_tasks,
+                                   double *d_out, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Split-precision engine (factored Green operator + CRT INT8 GEMMs).
  *
