@@ -280,10 +280,12 @@ class SplitEngine:
                                            self.status.data_ptr(), _native.stream_handle(stream)),
                       "rkb_split_contract")
 
-    def stream_tables(self, sink, stream=None) -> None:
+    def stream_tables(self, sink, stream=None, check: bool = True) -> None:
         """Compute the rows once, then each multipole's table into one of two
         rotating device buffers and hand it to ``sink(k, table, blocks, stream)``
-        (see ``tables.stream_tables``); the whole table is never held."""
+        (see ``tables.stream_tables``); the whole table is never held.  With
+        ``check=False`` nothing waits for the device (call ``check_status()``
+        once the stream's work is known to be done)."""
         s = stream if stream is not None else torch.cuda.current_stream()
         plan = self.dev.plan
         self.rows(s)
@@ -297,7 +299,9 @@ class SplitEngine:
             buf = bufs[gi % 2][:nk * nk]
             self._contract(self.grp_out_zero, t0, t1, buf, s)
             sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
-        self.check_status()
+        self._bufs = bufs  # kept alive until the caller has waited for the stream
+        if check:
+            self.check_status()
 
     def run(self, stream=None, upload: bool = True, check: bool = True) -> torch.Tensor:
         self.rows(stream)

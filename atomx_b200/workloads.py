@@ -151,8 +151,14 @@ def uneven_batch(seed: int = 3064, n_ions: int = 64) -> list[IonSpec]:
     return out
 
 
-def serving_requests(seed: int = 4200, n_requests: int = 64, rate_per_s: float = 200.0):
-    """(arrival_time_s, IonSpec) pairs of a seeded Poisson request stream."""
+def serving_requests(seed: int = 4200, n_requests: int = 64, rate_per_s: float = 200.0, max_ns: int = 200,
+                     max_orbitals: int = 300, max_kmax: int = 14):
+    """(arrival_time_s, IonSpec) pairs of a seeded Poisson request stream.
+
+    Defaults are the serving workload (Z 2..92, 30..200 B-splines, 10..300
+    spinors, k_max 2..14, sized as the Z=70 ion); the max_* arguments clip the
+    ranges for small test streams.
+    """
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -160,9 +166,9 @@ def serving_requests(seed: int = 4200, n_requests: int = 64, rate_per_s: float =
     for i in range(n_requests):
         t += float(rng.exponential(1.0 / rate_per_s))
         Z = int(rng.integers(2, 93))
-        ns = int(rng.integers(30, 201))
-        norb = int(rng.integers(10, 301))
-        kmax = int(rng.integers(2, 15))
+        ns = int(rng.integers(30, max_ns + 1))
+        norb = int(rng.integers(10, max_orbitals + 1))
+        kmax = int(rng.integers(2, max_kmax + 1))
         out.append((t, IonSpec(Z=Z, ns=ns, ks=9, n_gauss=8, r_min=1e-6, r_max=60.0,
                                shells=_spread(norb, kaps), k_max=kmax,
                                seed=int(rng.integers(0, 2**31)), name=f"request{i}")))

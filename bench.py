@@ -396,6 +396,8 @@ def run_gpu(args):
             "roofline": dom, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(), "wall_s": t_wall}
     line.update(extra)
+    if args.serve > 0 and engine == "split":
+        line["serve"] = serve_leg(args)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
@@ -458,6 +460,42 @@ def e2e_leg(ion, engine, args, world, k_max):
             "note": "slater_rk_tables(ion) from host coefficients; full table copied to pinned host memory"}
 
 
+def serve_leg(args) -> dict:
+    """The seeded Poisson request stream (rate 200/s) served by the
+    continuous-batching loop, split engine and plain FP64 engine in turn."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from atomx_b200 import workloads as W
+    from atomx_b200.serve import Request, SlaterServer
+    stream = W.serving_requests(n_requests=args.serve)
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
+        ions = list(ex.map(lambda ts: W.build_ion(ts[1]), stream))  # client-side data, not timed
+    out = {"requests": len(stream), "rate_per_s": 200.0, "arrival_span_s": stream[-1][0],
+           "sink": "device: per-(k, row) sums of every multipole table",
+           "note": "latency = last table delivered - arrival (server clock), realtime Poisson arrivals"}
+    for precision in ("split", "fp64"):
+        reqs = [Request(rid=i, ion=ion, k_max=spec.k_max, arrival=t)
+                for i, ((t, spec), ion) in enumerate(zip(stream, ions))]
+        warm = SlaterServer(precision=precision, max_inflight=1)
+        warm.serve([Request(rid=-1, ion=ions[0], k_max=stream[0][1].k_max)], realtime=False)
+        warm.close()
+        torch_sync()
+        server = SlaterServer(precision=precision, max_inflight=4)
+        rep = server.serve(reqs, realtime=True)
+        server.close()
+        torch_sync()
+        out[precision] = rep.summary()
+        errs = [repr(r.error) for r in reqs if r.error is not None]
+        if errs:
+            out[precision]["errors"] = errs[:3]
+    return out
+
+
+def torch_sync():
+    import torch
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -469,6 +507,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
+    ap.add_argument("--serve", type=int, default=32, help="requests in the serving leg (0 = skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
