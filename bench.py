@@ -96,44 +96,23 @@ def measured_peaks():
 
 
 def dist_setup(n_gpus):
-    import torch
-    import torch.distributed as dist
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
-    return rank, world, local
+    from atomx_b200 import replicas
+    return replicas.init("nccl")
 
 
 def allreduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from atomx_b200 import replicas
+    return replicas.reduce_max(x, world)
 
 
 def allreduce_sum(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from atomx_b200 import replicas
+    return replicas.reduce_sum(x, world)
 
 
 def barrier(world: int):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from atomx_b200 import replicas
+    replicas.barrier(world)
 
 
 # ------------------------------------------------------------- CPU baseline
@@ -321,7 +300,8 @@ def run_gpu(args):
     from atomx_b200 import workloads as W
 
     rank, world, local = dist_setup(args.gpus)
-    spec = W.ytterbium_scaleup(seed=2026 + rank)
+    from atomx_b200.replicas import replica_seed
+    spec = W.ytterbium_scaleup(seed=replica_seed(2026, rank))
     k_max = spec.k_max if args.k_max is None else args.k_max
     ion = W.build_ion(spec)
     dev = T.upload_ion(ion, k_max=k_max)
@@ -402,9 +382,8 @@ def run_gpu(args):
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
         print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from atomx_b200 import replicas
+    replicas.finalize(world)
     return 0
 
 
