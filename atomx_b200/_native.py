@@ -39,10 +39,12 @@ _SIGNATURES = {
     "rkb_split_rows_fused": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _l,
                              _l, _l, _vp, _vp, _vp, _vp, _i, _vp],
     "rkb_split_fused_body_width": [_i, _i],
+    "rkb_green_factor": [_vp, _i, _i, _i, _d, _vp, _vp, _vp, _l],
     "rkb_split_contract": [_vp, _vp, _l, _l, _i, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp,
                            _vp, _vp, _vp, _l, _vp, _vp, _vp],
 }
-_RESTYPE = {"rkb_last_error": _c.c_char_p, "rkb_version": _c.c_char_p, "rkb_split_fused_body_width": _c.c_long}
+_RESTYPE = {"rkb_last_error": _c.c_char_p, "rkb_version": _c.c_char_p, "rkb_split_fused_body_width": _c.c_long,
+            "rkb_green_factor": _c.c_long}
 
 _lock = threading.Lock()
 _lib = None

@@ -34,7 +34,7 @@ import torch
 from . import _native
 from .split import IonRows, _round_up, choose_width
 from .split_plan import crt_constants
-from .tables import IonDevice, RkTables, TILE
+from .tables import TILE, IonDevice, RkTables, tile_tasks
 
 __all__ = ["SplitBatch", "Fp64Batch", "batch_tasks"]
 
@@ -46,13 +46,7 @@ def batch_tasks(sizes, costs, order: str = "lpt") -> np.ndarray:
     contraction length). "lpt" puts the most expensive tiles first (persistent
     CTAs then finish close together); "group" keeps groups in order.
     """
-    out = []
-    for g, n in enumerate(sizes):
-        nt = (int(n) + TILE - 1) // TILE
-        for ti in range(nt):
-            for tj in range(ti, nt):
-                out.append((g, ti, tj))
-    tasks = np.asarray(out, dtype=np.int32).reshape(-1, 3)
+    tasks = tile_tasks(sizes)
     if order == "lpt" and tasks.shape[0]:
         c = np.asarray(costs, dtype=np.float64)[tasks[:, 0]]
         tasks = tasks[np.argsort(-c, kind="stable")]

@@ -1,0 +1,205 @@
+// Host-side planning for the split engine: the factored Green operator of one
+// multipole on one grid, packed as the device kernels read it.
+//
+// With u = r^-(k+1), v = r^k per node and the interpolatory partial matrices
+// mo, mi (mo + mi = 1) of the cell rule, atomx's Y^k (numerics/yk.py:88-154)
+// contracts to R = g^T G g with G's cell blocks u_i v_j mo_ij + v_i u_j mi_ij
+// (diagonal cells) and rank-one kernel samples off the diagonal.  The body
+// (cells >= 1) gets the structured modified Cholesky
+//     S_m = D_m - sigma u_m u_m^T,   L_m L_m^T = S_m + Delta_m,
+//     c_m = L_m^-1 (v_m - sigma u_m),  sigma += |c_m|^2,
+// where Delta_m = sum_e z_e z_e^T lifts every eigenvalue of the diagonally
+// scaled S_m below tau * lambda_max to max(|lambda|, tau lambda_max); the z_e
+// become the negative-sign columns Z.  Then ell_m = L_m^-1 u_m (1 - sum
+// c.ell) carries the core-body coupling, and S_c = G_00 - |ell|^2 v_0 v_0^T
+// is the FP64 core term.  This is the same factorisation as
+// atomx_b200.split_plan.green_factor (numpy); the eigenproblems here are
+// solved by cyclic Jacobi rotations (ng <= 32), so eigenvector signs may
+// differ, which leaves every z_e z_e^T and the factor unchanged.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "rkb_common.cuh"
+
+namespace rkb {
+namespace plan {
+
+// Symmetric eigenproblem A = V diag(w) V^T (n <= 32) by cyclic Jacobi.
+// A is overwritten; V is row-major with eigenvectors in columns.
+static void jacobi_eigh(int n, double *A, double *w, double *V) {
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) V[i * n + j] = i == j ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < n; ++i) {
+            diag += A[i * n + i] * A[i * n + i];
+            for (int j = i + 1; j < n; ++j) off += A[i * n + j] * A[i * n + j];
+        }
+        if (off <= 1e-34 * diag || off == 0.0) break;
+        for (int p = 0; p < n; ++p) {
+            for (int q = p + 1; q < n; ++q) {
+                const double apq = A[p * n + q];
+                if (apq == 0.0) continue;
+                const double app = A[p * n + p], aqq = A[q * n + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int i = 0; i < n; ++i) {  // A <- A J (columns p, q)
+                    const double aip = A[i * n + p], aiq = A[i * n + q];
+                    A[i * n + p] = c * aip - s * aiq;
+                    A[i * n + q] = s * aip + c * aiq;
+                }
+                for (int j = 0; j < n; ++j) {  // A <- J^T A (rows p, q)
+                    const double apj = A[p * n + j], aqj = A[q * n + j];
+                    A[p * n + j] = c * apj - s * aqj;
+                    A[q * n + j] = s * apj + c * aqj;
+                }
+                for (int i = 0; i < n; ++i) {  // V <- V J
+                    const double vip = V[i * n + p], viq = V[i * n + q];
+                    V[i * n + p] = c * vip - s * viq;
+                    V[i * n + q] = s * vip + c * viq;
+                }
+            }
+        }
+    }
+    for (int i = 0; i < n; ++i) w[i] = A[i * n + i];
+}
+
+// Lower Cholesky factor of an SPD matrix (row-major, in place below the
+// diagonal; the strict upper part is zeroed).  False if not positive.
+static bool cholesky(int n, double *A) {
+    for (int j = 0; j < n; ++j) {
+        double d = A[j * n + j];
+        for (int p = 0; p < j; ++p) d -= A[j * n + p] * A[j * n + p];
+        if (!(d > 0.0)) return false;
+        d = std::sqrt(d);
+        A[j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double s = A[i * n + j];
+            for (int p = 0; p < j; ++p) s -= A[i * n + p] * A[j * n + p];
+            A[i * n + j] = s / d;
+        }
+        for (int i = 0; i < j; ++i) A[i * n + j] = 0.0;
+    }
+    return true;
+}
+
+// x = L^-1 b (forward substitution, L lower, row-major).
+static void lower_solve(int n, const double *L, const double *b, double *x) {
+    for (int i = 0; i < n; ++i) {
+        double s = b[i];
+        for (int p = 0; p < i; ++p) s -= L[i * n + p] * x[p];
+        x[i] = s / L[i * n + i];
+    }
+}
+
+}  // namespace plan
+}  // namespace rkb
+
+using namespace rkb;
+
+extern "C" long rkb_green_factor(const double *r, int nv, int ng, int k, double tau, const double *mo,
+                                 const double *mi, double *out, long cap) {
+    RKB_CHECK_ARG(r != nullptr && mo != nullptr && mi != nullptr && out != nullptr, "null argument");
+    RKB_CHECK_ARG(nv >= 2 && ng >= 1 && ng <= RKB_MAX_NG, "invalid grid (nv=%d, ng=%d)", nv, ng);
+    RKB_CHECK_ARG(k >= 0 && tau >= 0.0, "invalid multipole or shift threshold");
+    const int n = nv * ng, g2 = ng * ng;
+    const long fixed = 2L * n + (long)nv * g2 + (long)nv * ng + ng + g2 + 1;
+    RKB_CHECK_ARG(cap >= fixed, "output capacity %ld below the %ld fixed doubles", cap, fixed);
+    std::vector<double> u(n), v(n), ell(n, 0.0), Lb((size_t)nv * g2, 0.0), C((size_t)nv * ng, 0.0);
+    for (int i = 0; i < n; ++i) {
+        u[i] = std::pow(r[i], -(double)(k + 1));
+        v[i] = std::pow(r[i], (double)k);
+    }
+    std::vector<double> D(g2), S(g2), A(g2), T(g2), V(g2), w(ng), d(ng), rhs(ng);
+    std::vector<int> zcell;
+    std::vector<double> zvec;
+    double sigma = 0.0;
+    for (int m = 1; m < nv; ++m) {
+        const double *um = &u[(size_t)m * ng], *vm = &v[(size_t)m * ng];
+        for (int i = 0; i < ng; ++i)
+            for (int j = 0; j < ng; ++j)
+                D[i * ng + j] = um[i] * vm[j] * mo[i * ng + j] + vm[i] * um[j] * mi[i * ng + j];
+        for (int i = 0; i < ng; ++i)
+            for (int j = 0; j < i; ++j) {
+                const double s = 0.5 * (D[i * ng + j] + D[j * ng + i]);
+                D[i * ng + j] = D[j * ng + i] = s;
+            }
+        for (int i = 0; i < ng; ++i) d[i] = std::sqrt(std::fabs(D[i * ng + i]));
+        for (int i = 0; i < ng; ++i)
+            for (int j = 0; j < ng; ++j) {
+                S[i * ng + j] = D[i * ng + j] - sigma * um[i] * um[j];
+                A[i * ng + j] = S[i * ng + j] / (d[i] * d[j]);
+            }
+        // Certificate that no eigenvalue needs a shift: with lambda_max <= gb
+        // (Gershgorin), a Cholesky of A - tau*gb*I proves lambda_min > tau*gb
+        // >= tau*lambda_max, and the eigensolve is skipped (most cells).
+        double gb = 0.0;
+        for (int i = 0; i < ng; ++i) {
+            double row = 0.0;
+            for (int j = 0; j < ng; ++j) row += std::fabs(A[i * ng + j]);
+            gb = std::fmax(gb, row);
+        }
+        std::memcpy(T.data(), A.data(), sizeof(double) * g2);
+        for (int i = 0; i < ng; ++i) T[i * ng + i] -= tau * gb;
+        const bool no_shift = tau > 0.0 && plan::cholesky(ng, T.data());
+        if (!no_shift) plan::jacobi_eigh(ng, A.data(), w.data(), V.data());
+        double lmax = no_shift ? 0.0 : w[0];
+        for (int e = 1; e < ng && !no_shift; ++e) lmax = std::fmax(lmax, w[e]);
+        const double floor = tau * lmax;
+        for (int e = 0; e < ng && !no_shift; ++e) {
+            if (!(w[e] < floor)) continue;
+            const double shift = std::fmax(std::fabs(w[e]), floor) - w[e];
+            const double sq = std::sqrt(shift);
+            zcell.push_back(m);
+            const size_t z0 = zvec.size();
+            for (int i = 0; i < ng; ++i) zvec.push_back(sq * V[i * ng + e] * d[i]);
+            for (int i = 0; i < ng; ++i)
+                for (int j = 0; j < ng; ++j) S[i * ng + j] += zvec[z0 + i] * zvec[z0 + j];
+        }
+        double *Lm = &Lb[(size_t)m * g2];
+        std::memcpy(Lm, S.data(), sizeof(double) * g2);
+        if (!plan::cholesky(ng, Lm)) {
+            set_error("green factor: cell %d of multipole %d is not positive after the shift", m, k);
+            return -(long)RKB_ENONFINITE;
+        }
+        for (int i = 0; i < ng; ++i) rhs[i] = vm[i] - sigma * um[i];
+        double *Cm = &C[(size_t)m * ng];
+        plan::lower_solve(ng, Lm, rhs.data(), Cm);
+        for (int i = 0; i < ng; ++i) sigma += Cm[i] * Cm[i];
+    }
+    double s_acc = 0.0, ell2 = 0.0;
+    for (int m = 1; m < nv; ++m) {
+        for (int i = 0; i < ng; ++i) rhs[i] = u[(size_t)m * ng + i] * (1.0 - s_acc);
+        double *em = &ell[(size_t)m * ng];
+        plan::lower_solve(ng, &Lb[(size_t)m * g2], rhs.data(), em);
+        for (int i = 0; i < ng; ++i) {
+            s_acc += C[(size_t)m * ng + i] * em[i];
+            ell2 += em[i] * em[i];
+        }
+    }
+    const long nz = (long)zcell.size();
+    const long total = fixed + nz * (ng + 1);
+    RKB_CHECK_ARG(cap >= total, "output capacity %ld below the %ld doubles of this factor", cap, total);
+    // u[N] | ell[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] | Sc[ng][ng] | nZ | nZ x (cell, z[ng])
+    double *o = out;
+    std::memcpy(o, u.data(), sizeof(double) * n); o += n;
+    std::memcpy(o, ell.data(), sizeof(double) * n); o += n;
+    std::memcpy(o, Lb.data(), sizeof(double) * (size_t)nv * g2); o += (size_t)nv * g2;
+    std::memcpy(o, C.data(), sizeof(double) * (size_t)nv * ng); o += (size_t)nv * ng;
+    for (int i = 0; i < ng; ++i) o[i] = v[i];
+    o += ng;
+    for (int i = 0; i < ng; ++i)
+        for (int j = 0; j < ng; ++j) {
+            const double gcc = u[i] * v[j] * mo[i * ng + j] + v[i] * u[j] * mi[i * ng + j];
+            o[i * ng + j] = gcc - ell2 * v[i] * v[j];
+        }
+    o += g2;
+    *o++ = (double)nz;
+    for (long e = 0; e < nz; ++e) {
+        *o++ = (double)zcell[e];
+        for (int i = 0; i < ng; ++i) *o++ = zvec[(size_t)e * ng + i];
+    }
+    return total;
+}

@@ -58,15 +58,12 @@ class TablePlan:
 
     def block_ranges_of_k(self, k: int):
         """[(block_id, start, stop)] row ranges of the k-th table."""
-        pk = self.pairs_of_k[k]
-        bid = self.pair_block[pk]
-        out = []
-        start = 0
-        for i in range(1, pk.shape[0] + 1):
-            if i == pk.shape[0] or bid[i] != bid[start]:
-                out.append((int(bid[start]), start, i))
-                start = i
-        return out
+        bid = self.pair_block[self.pairs_of_k[k]]
+        if bid.shape[0] == 0:
+            return []
+        starts = np.concatenate([[0], np.flatnonzero(bid[1:] != bid[:-1]) + 1])
+        stops = np.concatenate([starts[1:], [bid.shape[0]]])
+        return [(int(bid[a]), int(a), int(b)) for a, b in zip(starts, stops)]
 
 
 def make_plan(kappa, k_max: int) -> TablePlan:

@@ -12,12 +12,12 @@ R^k tables. The server runs each request through three stages:
    GPU, and while a stream slot is free. The footprint is the coefficients,
    orbital values, residue or (g, Y) rows, and the two rotating table
    buffers;
-3. device work, on the request's own CUDA stream: upload, orbital
-   evaluation, rows, and one multipole table after another, each handed to
-   the request's sink with its kappa-block ranges (``tables.stream_tables``).
-   An event after the last table marks completion; the server polls it,
-   checks the engine's device status, frees the request's memory and admits
-   the next one.
+3. device work, on the request's own CUDA stream and set up by the stream
+   slot's launcher thread: upload, orbital evaluation, rows, and one
+   multipole table after another, each handed to the request's sink with its
+   kappa-block ranges (``tables.stream_tables``). An event after the last
+   table marks completion. The server polls it, checks the engine's device
+   status, frees the request's memory and admits the next one.
 
 Requests that arrive while others are on the GPU are planned at once and
 admitted as slots and memory free up. Their kernels then overlap with the
@@ -129,7 +129,12 @@ class SlaterServer:
             free, total = torch.cuda.mem_get_info()
             hbm_budget = int(0.6 * free)
         self.hbm_budget = int(hbm_budget)
+        self.device = torch.cuda.current_device()
         self.pool = ThreadPoolExecutor(max_workers=workers)
+        # one launcher thread per stream slot: a request's uploads, engine
+        # set-up and launches run there, so requests prepare in parallel and
+        # the loop itself only admits and retires
+        self.launchers = ThreadPoolExecutor(max_workers=self.max_inflight)
         self.streams = [torch.cuda.Stream() for _ in range(self.max_inflight)]
 
     # ---------------------------------------------------------------- stages
@@ -146,7 +151,7 @@ class SlaterServer:
         from . import tables as T
         sink = req.sink if req.sink is not None else ChecksumSink()
         req.sink = sink
-        with torch.cuda.stream(stream):
+        with torch.cuda.device(self.device), torch.cuda.stream(stream):
             dev = upload_ion(req.ion, k_max=req.k_max, plan=req.plan, stream=stream)
             if self.precision == "split":
                 from .split import SplitEngine
@@ -162,10 +167,12 @@ class SlaterServer:
     def _finish(self, req: Request) -> None:
         eng = req.state.get("engine")
         try:
-            if eng is not None:
+            if eng is not None and req.error is None:
                 eng.check_status()
         except BaseException as exc:  # a failed request does not stop the server
             req.error = exc
+        # buffers allocated on the request's stream return to that stream's
+        # pool, so anything a failed launcher enqueued still runs first
         req.state.clear()
 
     # ------------------------------------------------------------------ loop
@@ -202,10 +209,18 @@ class SlaterServer:
             planning = still
             if len(ready) > 1:
                 ready = deque(sorted(ready, key=lambda r: r.arrival))
-            # completions
+            # completions (a request is done once its launcher has enqueued
+            # everything and the completion event has fired)
             for item in list(inflight):
                 r, s = item
-                if r.state["event"].query():
+                fut = r.state.get("launch")
+                if fut is not None:
+                    if not fut.done():
+                        continue
+                    del r.state["launch"]
+                    if fut.exception() is not None:
+                        r.error = fut.exception()
+                if r.error is not None or r.state["event"].query():
                     r.done = now()
                     self._finish(r)
                     used -= r.footprint
@@ -220,12 +235,7 @@ class SlaterServer:
                 ready.popleft()
                 s = free_streams.pop()
                 r.admitted = now()
-                try:
-                    self._launch(r, s)
-                except BaseException as exc:
-                    r.error, r.done = exc, now()
-                    free_streams.append(s)
-                    continue
+                r.state["launch"] = self.launchers.submit(self._launch, r, s)
                 used += r.footprint
                 inflight.append((r, s))
                 max_seen = max(max_seen, len(inflight))
@@ -240,3 +250,4 @@ class SlaterServer:
 
     def close(self):
         self.pool.shutdown(wait=True)
+        self.launchers.shutdown(wait=True)

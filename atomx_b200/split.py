@@ -26,7 +26,8 @@ import numpy as np
 import torch
 
 from . import _native
-from .split_plan import bits_for_moduli, crt_constants, green_factor, moduli_needed, pack_factors
+from .split_plan import (bits_for_moduli, concat_tables, crt_constants, green_factor_packed, moduli_needed,
+                         table_z_count)
 from .tables import IonDevice, tile_tasks
 
 __all__ = ["SplitEngine", "IonRows", "factors_for_grid", "choose_width", "DEFAULT_BITS"]
@@ -50,7 +51,8 @@ _factor_lock = threading.Lock()
 
 
 def factors_for_grid(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
-    """k -> factor dict for a grid (cached by grid content, k and tau)."""
+    """k -> packed factor table for a grid (native factorisation, cached by
+    grid content, k and tau)."""
     r_flat = np.ascontiguousarray(r_flat, dtype=np.float64)
     key0 = (hashlib.blake2b(r_flat.tobytes(), digest_size=16).hexdigest(), ng, tau)
     out = {}
@@ -59,9 +61,9 @@ def factors_for_grid(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict
         with _factor_lock:
             F = _factor_cache.get(key)
         if F is None:
-            F = green_factor(r_flat, ng, int(k), tau=tau)
+            F = green_factor_packed(r_flat, ng, int(k), tau=tau)
             with _factor_lock:
-                if len(_factor_cache) > 512:
+                if len(_factor_cache) > 4096:
                     _factor_cache.clear()
                 _factor_cache[key] = F
         out[int(k)] = F
@@ -118,7 +120,7 @@ class IonRows:
             r_host = dev.r.detach().cpu().numpy()
         self.factors = factors_for_grid(r_host, ng, plan.ks, tau=tau)
         kmax = max(plan.ks)
-        flat, offs = pack_factors([self.factors[k] for k in plan.ks])
+        flat, offs = concat_tables([self.factors[k] for k in plan.ks])
         koff = np.full(kmax + 1, -1, dtype=np.int64)
         for i, k in enumerate(plan.ks):
             koff[k] = offs[i]
@@ -126,7 +128,7 @@ class IonRows:
         self.ktab = torch.as_tensor(flat, device=d)
         self.koff = torch.as_tensor(koff, device=d)
         self.kbody = (nv - 1) * ng
-        self.nz = {k: int(self.factors[k]["zcell"].shape[0]) for k in plan.ks}
+        self.nz = {k: table_z_count(self.factors[k], nv, ng) for k in plan.ks}
         max_z = max(self.nz.values())
         fits = fused_fits(nv, ng, max_z)
         if fused and not fits:

@@ -60,7 +60,7 @@ import numpy as np
 from .yk import yk_partial_matrices
 
 __all__ = ["MODULI", "bits_for_moduli", "crt_constants", "digit_moduli", "moduli_needed", "green_factor",
-           "pack_factors", "factor_table_layout"]
+           "green_factor_packed", "pack_factors", "concat_tables", "table_z_count", "factor_table_layout"]
 
 #: Pairwise-coprime moduli, largest first (256 = 2^8; 255 = 3*5*17; 253 = 11*23;
 #: 247 = 13*19; 217 = 7*31; the rest are primes).
@@ -159,6 +159,36 @@ def green_factor(r_flat: np.ndarray, ng: int, k: int, tau: float = 1e-3) -> dict
     Sc = Gcc - float(np.sum(ell * ell)) * np.outer(v[0], v[0])
     return dict(k=k, nv=nv, ng=ng, u=u, v0=v[0].copy(), Lb=Lb, C=C, Gcc=Gcc, ell=ell, Sc=Sc,
                 zcell=np.asarray(zcell, dtype=np.int64), zvec=np.asarray(zvec).reshape(-1, ng))
+
+
+def green_factor_packed(r_flat: np.ndarray, ng: int, k: int, tau: float = 1e-3) -> np.ndarray:
+    """The same factorisation as ``green_factor``, computed natively and
+    returned packed (``pack_factors`` layout of one table)."""
+    from . import _native
+    L = _native.load()
+    r = np.ascontiguousarray(r_flat, dtype=np.float64)
+    nv = r.shape[0] // ng
+    mo, mi = yk_partial_matrices(ng)
+    mo = np.ascontiguousarray(mo, dtype=np.float64)
+    mi = np.ascontiguousarray(mi, dtype=np.float64)
+    cap = 2 * nv * ng + nv * ng * ng + nv * ng + ng + ng * ng + 1 + nv * ng * (ng + 1)
+    out = np.empty(cap, dtype=np.float64)
+    got = L.rkb_green_factor(r.ctypes.data, nv, ng, int(k), float(tau), mo.ctypes.data, mi.ctypes.data,
+                             out.ctypes.data, cap)
+    if got < 0:
+        _native.check(int(-got), "rkb_green_factor")
+    return out[:got].copy()
+
+
+def table_z_count(table: np.ndarray, nv: int, ng: int) -> int:
+    """Number of Z columns of one packed factor table."""
+    return int(table[factor_table_layout(nv, ng)["nz"]])
+
+
+def concat_tables(tables: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray]:
+    """Concatenate packed tables: (flat doubles, offsets by list index)."""
+    offs = np.concatenate([[0], np.cumsum([t.shape[0] for t in tables])])[:-1].astype(np.int64)
+    return np.concatenate(tables), offs
 
 
 def factor_table_layout(nv: int, ng: int) -> dict:

@@ -110,13 +110,14 @@ def upload_values(Pv, Qv, kappa, gr, grw, k_max: int, plan: TablePlan | None = N
 
 def tile_tasks(sizes, tile: int = TILE):
     """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes."""
-    out = []
+    parts = []
     for g, n in enumerate(sizes):
         nt = (int(n) + tile - 1) // tile
-        for ti in range(nt):
-            for tj in range(ti, nt):
-                out.append((g, ti, tj))
-    return np.asarray(out, dtype=np.int32).reshape(-1, 3)
+        ti, tj = np.triu_indices(nt)
+        parts.append(np.stack([np.full(ti.shape[0], g), ti, tj], axis=1))
+    if not parts:
+        return np.zeros((0, 3), dtype=np.int32)
+    return np.concatenate(parts).astype(np.int32).reshape(-1, 3)
 
 
 @dataclass

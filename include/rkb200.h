@@ -189,6 +189,17 @@ int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long orb_ld, co
                          long kpad, long row_base, long nrows_total, double *d_rowscale,
                          double *d_left, double *d_right, double *d_cbound, int cwp, void *stream);
 
+/* Host-only planning (no device work): the packed factored Green operator of
+ * multipole k on the grid r (nv cells x ng nodes, mo/mi the ng x ng partial
+ * matrices of atomx numerics/yk.py:65 yk_partial_matrices) with eigenvalue
+ * shift threshold tau, in the layout rkb_split_rows reads (d_ktab):
+ * u[N] | ell[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] | Sc[ng][ng] | nZ |
+ * nZ x (cell, z[ng]).  Writes at most cap doubles to out; returns the count
+ * written or a negative rkb_status.  atomx has no counterpart (its Y^k is
+ * a scan, numerics/yk.py:88; this factors the same operator). */
+long rkb_green_factor(const double *r, int nv, int ng, int k, double tau, const double *mo,
+                      const double *mi, double *out, long cap);
+
 /* Residue positions spanned by the body in rkb_split_rows_fused's layout (a
  * multiple of 128), or -1 for an invalid grid.  Host-only, no device work. */
 long rkb_split_fused_body_width(int nv, int ng);

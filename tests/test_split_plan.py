@@ -23,12 +23,12 @@ def _ion_rows(name, n_pairs=120, seed=0):
 @pytest.mark.parametrize("name,ks", [("neon_small", [0, 1, 2]), ("ytterbium_scaleup", [0, 5, 12])])
 def test_factored_identity_matches_oracle(name, ks):
     from atomx_b200.split import factors_for_grid
-    from atomx_b200.split_plan import pack_factors
+    from atomx_b200.split_plan import concat_tables
     spec, ion, bd, Pg, Qg, plan = _ion_rows(name)
     gr, grw = bd["gr"], bd["grw"]
     nv, ng = gr.shape
     facs = factors_for_grid(gr.ravel(), ng, ks)
-    flat, offs = pack_factors([facs[k] for k in ks])
+    flat, offs = concat_tables([facs[k] for k in ks])
     rng = np.random.default_rng(1)
     for i, k in enumerate(ks):
         F = unpack_table(flat, offs[i], nv, ng)
@@ -70,8 +70,7 @@ def test_fixed_point_split_error_model():
     gr, grw = bd["gr"], bd["grw"]
     nv, ng = gr.shape
     for k in (0, 12):
-        F = factors_for_grid(gr.ravel(), ng, [k])[k]
-        F = dict(F, zcell=F["zcell"], zvec=F["zvec"])
+        F = unpack_table(factors_for_grid(gr.ravel(), ng, [k])[k], 0, nv, ng)
         pk = plan.pairs_of_k[k]
         sel = pk[np.random.default_rng(k).choice(pk.shape[0], size=min(200, pk.shape[0]), replace=False)]
         rho = np.array([Pg[a] * Pg[c] + Qg[a] * Qg[c] for a, c in plan.pairs[sel]])
@@ -88,3 +87,26 @@ def test_fixed_point_split_error_model():
         d = np.abs(np.diag(ref))
         err = np.abs(got - ref) / np.sqrt(np.outer(d, d))
         assert err.max() < 5e-11, (k, err.max())
+
+
+@pytest.mark.parametrize("name,ks", [("neon_small", [0, 1, 2]), ("ytterbium_scaleup", [0, 3, 12]),
+                                     ("xenon_ci_table", [0, 16])])
+def test_native_factor_equals_numpy_factor(name, ks):
+    """The native factorisation (Jacobi eigensolver) and the numpy one give the
+    same packed table; Z columns may differ in sign only (z z^T is the same)."""
+    from atomx_b200.split_plan import green_factor, green_factor_packed, pack_factors
+    spec, ion, bd, Pg, Qg, plan = _ion_rows(name)
+    nv, ng = bd["gr"].shape
+    r = bd["gr"].ravel()
+    for k in ks:
+        a = unpack_table(green_factor_packed(r, ng, k), 0, nv, ng)
+        ref_flat, _ = pack_factors([green_factor(r, ng, k)])
+        b = unpack_table(ref_flat, 0, nv, ng)
+        for key in ("u", "ell", "Lb", "C", "v0", "Sc"):
+            scale = np.abs(b[key]).max() + 1e-300
+            assert np.abs(a[key] - b[key]).max() <= 1e-11 * scale, (name, k, key)
+        np.testing.assert_array_equal(a["zcell"], b["zcell"])
+        for m in np.unique(b["zcell"]):
+            za, zb = a["zvec"][a["zcell"] == m], b["zvec"][b["zcell"] == m]
+            pa, pb = za.T @ za, zb.T @ zb
+            assert np.abs(pa - pb).max() <= 1e-10 * (np.abs(pb).max() + 1e-300), (name, k, m)
