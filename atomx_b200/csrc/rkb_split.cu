@@ -13,12 +13,13 @@
 //      x~ and writes int8 residues x~ mod m_i (and the B copy with Z negated)
 //      in a [modulus][row][kpad] layout, one 16-byte store per modulus.
 //
-// K3s  crt_syrk_kernel  (persistent, one CTA per SM, 10 warps)
+// K3s  crt_syrk_kernel  (persistent, one CTA per SM, 18 warps)
 //      warp 0: TMA producer — 128x128-byte boxes (SWIZZLE_128B) of the A and B
 //              residue matrices into a STAGES-deep ring;
 //      warp 1: TMEM owner + MMA issuer — tcgen05.mma.kind::i8, M=N=128, K=32,
 //              int32 accumulators in a double-buffered TMEM tile;
-//      warps 2-9: epilogue (4 TMEM lane quarters x 2 column halves) — per
+//      warps 2-17: epilogue (4 TMEM lane quarters x 4 column groups; four
+//              warps per SM sub-partition hide the TMEM and ALU latency) — per
 //              modulus: TMEM -> registers, reduce to [0, m) with integer
 //              operations, merge each even/odd pair of moduli into a 16-bit
 //              digit mod m_e m_o (two digits per 32-bit word; words of four
@@ -476,10 +477,10 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
 // K3s — tcgen05 INT8 residue SYRK with CRT epilogue
 // =========================================================================
 constexpr int BM = 128, BN = 128, BKB = 128;  // tile rows, tile cols, K bytes per stage
-constexpr int STAGES = 5;
+constexpr int STAGES = 4;
 constexpr int STAGE_BYTES = (BM + BN) * BKB;  // 32 KB
-constexpr int EPI_WARPS = 8;                  // 4 TMEM lane quarters x 2 column halves
-constexpr int EPI_COLS = BN / 2;              // columns per epilogue thread
+constexpr int EPI_WARPS = 16;                 // 4 TMEM lane quarters x 4 column groups
+constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // columns per epilogue thread
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
 constexpr int STG_LD = 17;  // doubles per staged row (16 + pad)
 constexpr size_t SMEM_BYTES = 1024 /*align slack*/ + (size_t)STAGES * STAGE_BYTES +
@@ -694,10 +695,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ------------------------------------------------------------ epilogue
         const int ew = warp - 2;
         const int quarter = warp & 3;       // TMEM lane quarter this warp may access
-        const int half = ew >> 2;           // column half of the tile
+        const int cgrp = ew >> 2;           // column group of the tile
         const int rloc = quarter * 32 + lane;
         const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-        const uint32_t col0 = (uint32_t)(half * EPI_COLS);
+        const uint32_t col0 = (uint32_t)(cgrp * EPI_COLS);
         double *stg = stage_out + (size_t)ew * 32 * STG_LD;
         uint32_t acc_it = 0;
         bool ok = true;
@@ -765,14 +766,14 @@ __global__ void __launch_bounds__(THREADS, 1)
             const double *la = p.left + (row0 + (arow ? a : 0)) * p.cwp;
             const bool mirror = ti != tj;
             double *R = p.out + p.grp_out[g];
-            // Correction screen for this warp's 32 x 64 block: with per-row bounds
+            // Correction screen for this warp's 32 x EPI_COLS block: with per-row bounds
             // relative to each row's scale, |left_a . right_b| <= 2^(e_a+e_b) *
             // |g0_a| |S_c g0_b|.  Below corr_floor the term is far under the
             // split's own error and is skipped.
             double r1 = 0.0, c2 = 0.0;
             if (arow) r1 = __ldg(p.cbound + (row0 + a) * 2);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < EPI_COLS / 32; ++h) {
                 const long bcol = b0 + lane + 32 * h;
                 if (bcol < n) c2 = fmax(c2, __ldg(p.cbound + (row0 + bcol) * 2 + 1));
             }
