@@ -32,7 +32,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .split import IonRows, _round_up, choose_width
+from .split import IonRows, _round_up, check_kdim, choose_width
 from .split_plan import crt_constants
 from .tables import TILE, IonDevice, RkTables, tile_tasks
 
@@ -92,6 +92,7 @@ class SplitBatch(_Graphable):
         self.ions = [IonRows(d, tau=tau, fused=fused) for d in self.devs]
         d = self.devs[0].Pv.device
         self.kpad = max(r.kmax_dim for r in self.ions)
+        check_kdim(self.kpad)
         self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
         self.cw = max(dv.ng for dv in self.devs)

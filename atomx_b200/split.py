@@ -37,6 +37,17 @@ __all__ = ["SplitEngine", "IonRows", "factors_for_grid", "choose_width", "DEFAUL
 DEFAULT_BITS = 36
 
 
+#: longest contraction the CRT kernel takes: its int32 accumulators are made
+#: nonnegative by a bias of m * 2^18 >= kdim * 128^2 for every modulus m >= 223
+KDIM_MAX = 3456
+
+
+def check_kdim(kdim: int) -> None:
+    if kdim > KDIM_MAX:
+        raise ValueError(f"grid too long for the split engine: contraction length {kdim} > {KDIM_MAX} "
+                         "(use precision='fp64')")
+
+
 def choose_width(bits, n_mod, kdim: int) -> tuple[int, int]:
     """(bits, n_mod) for a contraction length: explicit values are kept;
     bits=None takes the fewest moduli for DEFAULT_BITS and the widest split
@@ -206,6 +217,7 @@ class SplitEngine:
         self.fused, self.max_z, self.body_w, self.kdim, self.zcount = R.fused, R.max_z, R.body_w, R.kdim, R.zcount
         d = dev.Pv.device
         self.kpad = max(self.kdim.values())
+        check_kdim(self.kpad)
         self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
         self.cw = ng
