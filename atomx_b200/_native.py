@@ -38,6 +38,8 @@ _SIGNATURES = {
                                _l, _l, _vp, _vp, _vp, _vp, _i, _vp, _vp],
     "rkb_split_rows_fused": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _l,
                              _l, _l, _vp, _vp, _vp, _vp, _i, _vp],
+    "rkb_split_rows_cells": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _i, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp,
+                             _vp, _l, _l, _l, _vp, _vp, _vp, _vp, _i, _vp],
     "rkb_split_fused_body_width": [_i, _i],
     "rkb_green_factor": [_vp, _i, _i, _i, _d, _vp, _vp, _vp, _l],
     "rkb_split_contract": [_vp, _vp, _l, _l, _i, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp,

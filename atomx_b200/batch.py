@@ -107,7 +107,7 @@ class SplitBatch(_Graphable):
         self.left = torch.zeros((nrows, self.cwp), dtype=torch.float64, device=d)
         self.right = torch.zeros_like(self.left)
         self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
-        two = [dv.plan.n_rows for dv, r in zip(self.devs, self.ions) if not r.fused]
+        two = [dv.plan.n_rows for dv, r in zip(self.devs, self.ions) if r.kind == "two"]
         self.xwork = torch.empty((max(two), self.kpad), dtype=torch.float64, device=d) if two else None
         self.corr_floor = 2.0 ** -(self.bits + 10) if corr_floor is None else float(corr_floor)
         # groups: (ion, k)
@@ -137,7 +137,7 @@ class SplitBatch(_Graphable):
 
     @property
     def launches_per_step(self) -> int:
-        return sum(1 if r.fused else 2 for r in self.ions) + 1
+        return sum(2 if r.kind == "two" else 1 for r in self.ions) + 1
 
     @property
     def ordered_entries(self) -> int:
@@ -188,7 +188,8 @@ class SplitBatch(_Graphable):
     def info(self) -> dict:
         return {"ions": len(self.devs), "bits": self.bits, "n_mod": self.n_mod, "kpad": self.kpad,
                 "order": self.order, "tasks": self.n_tasks, "rows": int(self.row_base[-1]),
-                "fused_ions": int(sum(r.fused for r in self.ions)), "entries": self.ordered_entries}
+                "row_kernels": {kd: sum(r.kind == kd for r in self.ions) for kd in ("cells", "fused", "two")},
+                "entries": self.ordered_entries}
 
 
 class Fp64Batch(_Graphable):

@@ -473,6 +473,203 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Cell-parallel row kernel: one block per row, one thread per cell.  Thread t
+// owns cell m = nv-1-t (cells last to first), so a forward exclusive block
+// scan of the cell dots u_m.g_m gives each cell its suffix sum t_m directly.
+// The block first forms g = w*rho for the whole row with coalesced loads
+// (consecutive threads, consecutive nodes) into a padded shared-memory image;
+// each thread then reads its cell's g and the cell-minor factor copy
+// (entry i of every cell contiguous, so a warp's reads are consecutive) and
+// forms X = L_m^T g_m + C_m t_m + ell_m alpha in registers, without shuffles.
+// Threads past the cells compute the Z columns.  After a block maximum fixes
+// the row's power-of-two scale, every thread writes its int8 residues into
+// per-modulus row images in shared memory, and the block copies them out with
+// 16-byte stores.  Columns are in natural order: (m-1)*ng + node, then Z.
+//
+// Cell-minor factor table of one multipole (doubles), nv cells:
+//   u[NG][nv] | ell[NG][nv] | C[NG][nv] | L[NG][NG][nv] (L[i][node][m])
+template <int NG>
+__global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const double *__restrict__ ktab_t,
+                                                              const long *__restrict__ koff_t) {
+    constexpr int GS = NG | 1;  // padded cell stride of the g image (odd: 2-way bank conflicts at most)
+    extern __shared__ __align__(16) unsigned char smc[];
+    const int nv = a.nv;
+    const long q = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+    const long kpad = a.kpad;
+    const size_t ndbl = ((size_t)nv * GS + 66 + 1) & ~(size_t)1;     // doubles before the images (even: 16-B aligned)
+    double *gimg = reinterpret_cast<double *>(smc);                  // [nv][GS]
+    double *red = gimg + (size_t)nv * GS;                              // [64] block scratch
+    double *bcast = red + 64;                                          // alpha
+    unsigned char *lines = smc + ndbl * sizeof(double);               // [n_mod][kpad]
+    unsigned char *zneg = lines + (size_t)a.n_mod * kpad;             // [n_mod][64]: B's Z bytes
+    const int k = a.row_k[q];
+    const long pr = a.row_pair[q];
+    const double *Pa = a.P + a.pairs[2 * pr] * a.orb_ld, *Pc = a.P + a.pairs[2 * pr + 1] * a.orb_ld;
+    const double *Qa = a.Q + a.pairs[2 * pr] * a.orb_ld, *Qc = a.Q + a.pairs[2 * pr + 1] * a.orb_ld;
+    const long n = (long)nv * NG;
+    const double *tab = a.ktab + a.koff[k];
+    const double *v0 = tab + 2 * n + (long)nv * NG * NG + (long)nv * NG;
+    const double *Sc = v0 + NG;
+    const int nz = (int)Sc[NG * NG];
+    const double *zt = Sc + NG * NG + 1;
+    const double *tt = ktab_t + koff_t[k];
+    const double *ut = tt, *ellt = tt + n, *Ct = tt + 2 * n, *Lt = tt + 3 * n;
+    const long kbody = (long)(nv - 1) * NG;
+    const long grow = a.row_base + q;
+    // g = w * (P_a P_c + Q_a Q_c) for the whole row, coalesced
+    for (long j = tid; j < n; j += blockDim.x) {
+        const long cell = j / NG, node = j - cell * NG;
+        gimg[cell * GS + node] =
+            __dmul_rn(a.w[j], __dadd_rn(__dmul_rn(Pa[j], Pc[j]), __dmul_rn(Qa[j], Qc[j])));
+    }
+    __syncthreads();
+    const int m = nv - 1 - tid;  // this thread's cell (m < 0: a Z column or idle)
+    double g[NG], x[NG];
+    double d = 0.0;
+    if (m >= 0) {
+#pragma unroll
+        for (int i = 0; i < NG; ++i) g[i] = gimg[(long)m * GS + i];
+        if (m >= 1) {
+#pragma unroll
+            for (int i = 0; i < NG; ++i) d = fma(ut[(long)i * nv + m], g[i], d);
+        }
+    }
+    // cell 0: alpha = v_0 . g_0, core vectors and their norms (one thread)
+    double n1 = 0.0, n2 = 0.0;
+    if (m == 0) {
+        double al = 0.0;
+#pragma unroll
+        for (int i = 0; i < NG; ++i) al = fma(v0[i], g[i], al);
+        *bcast = al;
+#pragma unroll
+        for (int i = 0; i < NG; ++i) {
+            double sacc = 0.0;
+#pragma unroll
+            for (int j = 0; j < NG; ++j) sacc = fma(Sc[i * NG + j], g[j], sacc);
+            a.left[grow * a.cwp + i] = g[i];
+            a.right[grow * a.cwp + i] = sacc;
+            n1 = fma(g[i], g[i], n1);
+            n2 = fma(sacc, sacc, n2);
+        }
+        for (int i = NG; i < a.cwp; ++i) a.left[grow * a.cwp + i] = a.right[grow * a.cwp + i] = 0.0;
+    }
+    // exclusive scan of d over threads (= suffix sums over cells)
+    const double incl = warp_inclusive_scan(d, lane);
+    if (lane == 31) red[wid] = incl;
+    __syncthreads();
+    double before = 0.0;
+    for (int w = 0; w < wid; ++w) before += red[w];
+    const double up = __shfl_up_sync(0xffffffffu, incl, 1);
+    const double t_m = lane == 0 ? before : before + up;
+    const double alpha = *bcast;
+    double amax = 0.0;
+    bool bad = false;
+    if (m >= 1) {
+#pragma unroll
+        for (int node = 0; node < NG; ++node) {
+            double xv = fma(ellt[(long)node * nv + m], alpha, Ct[(long)node * nv + m] * t_m);
+#pragma unroll
+            for (int i = node; i < NG; ++i) xv = fma(Lt[((long)i * NG + node) * nv + m], g[i], xv);
+            x[node] = xv;
+            amax = fmax(amax, fabs(xv));
+            bad |= !isfinite(xv);
+        }
+    }
+    // Z columns: thread nv + e
+    const int e = tid - nv;
+    double zx = 0.0;
+    if (e >= 0 && e < nz) {
+        const double *ze = zt + (long)e * (NG + 1);
+        const long cz = (long)ze[0];
+#pragma unroll
+        for (int i = 0; i < NG; ++i) zx = fma(ze[1 + i], gimg[cz * GS + i], zx);
+        amax = fmax(amax, fabs(zx));
+        bad |= !isfinite(zx);
+    }
+    // block maximum and non-finite flag
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const int badw = __any_sync(0xffffffffu, bad);
+    __syncthreads();  // red[] reused
+    if (lane == 0) {
+        red[wid] = amax;
+        red[32 + wid] = badw ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    amax = 0.0;
+    bool anybad = false;
+    for (int w = 0; w < nwarp; ++w) {
+        amax = fmax(amax, red[w]);
+        anybad |= red[32 + w] != 0.0;
+    }
+    int ex = 0;
+    double scale = 0.0, inv_scale = 0.0;
+    if (!anybad && amax > 0.0) {
+        frexp(amax, &ex);  // amax < 2^ex
+        scale = ldexp(1.0, a.bits - ex);
+        inv_scale = ldexp(1.0, ex - a.bits);
+    }
+    if (m == 0) {
+        a.rowscale[grow] = anybad ? __longlong_as_double(0x7ff8000000000000LL) : inv_scale;
+        const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
+        a.cbound[grow * 2] = sqrt(n1) * rel;
+        a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+    }
+    // residues into the row images (natural column order), zero tails
+    const double rc = 6755399441055744.0;  // 1.5 * 2^52
+    const long zend = kbody + nz;
+    for (long c = zend + tid; c < kpad; c += blockDim.x)
+        for (int md = 0; md < a.n_mod; ++md) lines[(size_t)md * kpad + c] = 0;
+    if (m >= 1) {
+#pragma unroll
+        for (int node = 0; node < NG; ++node) x[node] = __dadd_rn(__fma_rn(x[node], scale, rc), -rc);
+        for (int md = 0; md < a.n_mod; ++md) {
+            const double mm = (double)a.mod[md], im = a.inv_mod[md];
+            unsigned char *ln = lines + (size_t)md * kpad + (long)(m - 1) * NG;
+#pragma unroll
+            for (int node = 0; node < NG; ++node) ln[node] = (unsigned char)residue_f64(x[node], mm, im);
+        }
+    }
+    if (e >= 0 && e < nz) {
+        zx = __dadd_rn(__fma_rn(zx, scale, rc), -rc);
+        for (int md = 0; md < a.n_mod; ++md) {
+            const uint32_t r = residue_f64(zx, (double)a.mod[md], a.inv_mod[md]);
+            lines[(size_t)md * kpad + kbody + e] = (unsigned char)r;
+            int nr = -(int)(int8_t)(uint8_t)r;  // residue of -x, centred again
+            nr -= nr > 127 ? a.mod[md] : 0;
+            zneg[md * 64 + e] = (unsigned char)nr;
+        }
+    }
+    __syncthreads();
+    // copy the row images out: 16-byte chunks; B's chunks that hold Z columns
+    // take their bytes from the negated copy
+    const long chunks = kpad / 16;
+    const long zc0 = kbody / 16, zc1 = (zend + 15) / 16;
+    for (long it = tid; it < (long)a.n_mod * chunks; it += blockDim.x) {
+        const int md = (int)(it / chunks);
+        const long ch = it - (long)md * chunks;
+        const uint4 v = *reinterpret_cast<const uint4 *>(lines + (size_t)md * kpad + ch * 16);
+        const long o = ((long)md * a.nrows_total + grow) * kpad + ch * 16;
+        *reinterpret_cast<uint4 *>(a.resA + o) = v;
+        if (a.resB) {
+            if (nz > 0 && ch >= zc0 && ch < zc1) {
+                unsigned char tmp[16];
+                *reinterpret_cast<uint4 *>(tmp) = v;
+                for (int b = 0; b < 16; ++b) {
+                    const long c = ch * 16 + b;
+                    if (c >= kbody && c < zend) tmp[b] = zneg[md * 64 + (c - kbody)];
+                }
+                *reinterpret_cast<uint4 *>(a.resB + o) = *reinterpret_cast<const uint4 *>(tmp);
+            } else {
+                *reinterpret_cast<uint4 *>(a.resB + o) = v;
+            }
+        }
+    }
+}
+
 // =========================================================================
 // K3s — tcgen05 INT8 residue SYRK with CRT epilogue
 // =========================================================================
@@ -969,6 +1166,60 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
     const long nthreads = nrows * (kpad / 16);
     split_residues_kernel<<<(unsigned)ceil_div(nthreads, 256), 256, 0, st>>>(a, d_zcount);
     RKB_LAUNCHED("split_residues_kernel");
+    return RKB_OK;
+}
+
+extern "C" int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                                    const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                                    int nv, int ng, const double *d_ktab, const long *d_koff,
+                                    const double *d_ktab_t, const long *d_koff_t, int max_z, int bits,
+                                    int n_mod, const int *moduli, signed char *d_resA, signed char *d_resB,
+                                    long kpad, long row_base, long nrows_total, double *d_rowscale, double *d_left,
+                                    double *d_right, double *d_cbound, int cwp, void *stream) {
+    RKB_CHECK_ARG(nv >= 2 && ng >= 5 && ng <= 11, "the cell row kernel takes 5 <= ng <= 11 (got %d)", ng);
+    RKB_CHECK_ARG(max_z >= 0 && max_z <= 64, "the cell row kernel takes <= 64 Z columns (got %d)", max_z);
+    const long threads = ((long)nv + max_z + 31) / 32 * 32;
+    RKB_CHECK_ARG(threads <= 256, "grid too long for the cell row kernel (%d cells + %d Z columns > 256)", nv,
+                  max_z);
+    RKB_CHECK_ARG(bits >= 8 && bits <= 40, "bits must be in [8, 40] (got %d)", bits);
+    RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
+    RKB_CHECK_ARG(kpad % BKB == 0 && kpad >= (long)(nv - 1) * ng + max_z, "kpad must be a multiple of %d >= %ld",
+                  BKB, (long)(nv - 1) * ng + max_z);
+    RKB_CHECK_ARG(cwp >= ng, "correction width must be >= ng");
+    RKB_CHECK_ARG(d_cbound != nullptr, "the correction-bound array is required");
+    RKB_CHECK_ARG(row_base >= 0 && row_base + nrows <= nrows_total, "row range outside the residue matrices");
+    RKB_CHECK_ARG(((uintptr_t)d_resA % 16) == 0 && (d_resB == nullptr || ((uintptr_t)d_resB % 16) == 0),
+                  "residue buffers must be 16-byte aligned");
+    if (nrows == 0) return RKB_OK;
+    RowsArgs a = {};
+    a.P = d_Pv; a.Q = d_Qv; a.orb_ld = orb_ld; a.pairs = d_pairs; a.row_pair = d_row_pair; a.row_k = d_row_k;
+    a.nrows = nrows; a.w = d_w; a.nv = nv; a.ng = ng; a.ktab = d_ktab; a.koff = d_koff; a.bits = bits;
+    a.n_mod = n_mod;
+    for (int i = 0; i < MAXMOD; ++i) {
+        const int m = i < n_mod ? moduli[i] : 256;
+        RKB_CHECK_ARG(m >= 2 && m <= 256, "moduli must lie in [2, 256]");
+        a.mod[i] = m;
+        a.inv_mod[i] = 1.0 / (double)m;
+    }
+    a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
+    a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
+    RKB_CHECK_ARG(d_ktab_t != nullptr && d_koff_t != nullptr, "the cell-minor factor tables are required");
+    const size_t smem = ((((size_t)nv * (ng | 1) + 66 + 1) & ~(size_t)1) * sizeof(double)) + (size_t)n_mod * (kpad + 64);
+    RKB_CHECK_ARG(smem <= 200 * 1024, "row images too large for shared memory");
+    cudaStream_t st = as_stream(stream);
+    const dim3 grid((unsigned)nrows), block((unsigned)threads);
+#define RKB_CELL_CASE(NGV)                                                         \
+    case NGV:                                                                      \
+        RKB_CUDA(set_smem(split_rows_cell_kernel<NGV>, (int)smem));                \
+        split_rows_cell_kernel<NGV><<<grid, block, smem, st>>>(a, d_ktab_t, d_koff_t); \
+        break;
+    switch (ng) {
+        RKB_CELL_CASE(5) RKB_CELL_CASE(6) RKB_CELL_CASE(7) RKB_CELL_CASE(8) RKB_CELL_CASE(9) RKB_CELL_CASE(10)
+        default:
+            RKB_CELL_CASE(11)
+    }
+#undef RKB_CELL_CASE
+    RKB_LAUNCHED("split_rows_cell_kernel");
     return RKB_OK;
 }
 

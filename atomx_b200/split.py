@@ -90,6 +90,12 @@ def fused_fits(nv: int, ng: int, max_z: int) -> bool:
     return 5 <= ng <= 11 and -(-(nv - 1) // (32 // ng)) <= FUSED_PASSES_MAX and max_z <= FUSED_Z_MAX
 
 
+def cells_fit(nv: int, ng: int, max_z: int) -> bool:
+    """Whether the cell-parallel row kernel takes this grid (one block of at
+    most 256 threads: a thread per cell plus one per Z column)."""
+    return 5 <= ng <= 11 and max_z <= 64 and -(-(nv + max_z) // 32) * 32 <= 256
+
+
 def fused_body_width(nv: int, ng: int) -> int:
     """Residue positions spanned by the body in the fused layout (multiple of 128)."""
     passes = -(-(nv - 1) // (32 // ng))
@@ -122,7 +128,7 @@ class IonRows:
 
     KCHUNK = 128
 
-    def __init__(self, dev: IonDevice, tau: float = 1e-3, fused: bool | None = None):
+    def __init__(self, dev: IonDevice, tau: float = 1e-3, fused: bool | None = None, rows_kernel: str | None = None):
         self.dev = dev
         plan = dev.plan
         nv, ng = dev.nv, dev.ng
@@ -145,15 +151,50 @@ class IonRows:
         if fused and not fits:
             raise ValueError(f"the fused row kernel does not fit this grid (nv={nv}, ng={ng}, Z columns {max_z})")
 
-        # rows in one register-resident kernel (permuted residue columns) or in
-        # two kernels through an FP64 workspace (columns in natural order); by
-        # default the fused kernel unless its layout adds more than 5 % to the
-        # GEMM work (sum over k of n_k^2 * kdim_k)
+        # Three row kernels write the same residues:
+        # * "cells": one block per row, one thread per cell (natural column
+        #   order); the default wherever it fits;
+        # * "fused": one warp per row in registers (permuted columns);
+        # * "two": rows to an FP64 workspace, then residues (natural order).
         def gemm_work(body):
             return sum(plan.n_of_k(k) ** 2 * _round_up(body + self.nz[k], self.KCHUNK) for k in plan.ks)
 
-        cheap = fits and gemm_work(fused_body_width(nv, ng)) <= 1.05 * gemm_work(self.kbody)
-        self.fused = cheap if fused is None else bool(fused)
+        if fused is not None:
+            kind = "fused" if fused else "two"
+        elif rows_kernel is not None:
+            kind = rows_kernel
+        elif cells_fit(nv, ng, max_z):
+            kind = "cells"
+        elif fits and gemm_work(fused_body_width(nv, ng)) <= 1.05 * gemm_work(self.kbody):
+            kind = "fused"
+        else:
+            kind = "two"
+        if kind not in ("cells", "fused", "two"):
+            raise ValueError(f"unknown row kernel {kind!r}")
+        if kind == "cells" and not cells_fit(nv, ng, max_z):
+            raise ValueError(f"the cell row kernel does not fit this grid (nv={nv}, ng={ng}, Z columns {max_z})")
+        if kind == "fused" and not fits:
+            raise ValueError(f"the fused row kernel does not fit this grid (nv={nv}, ng={ng}, Z columns {max_z})")
+        self.kind = kind
+        self.fused = kind == "fused"
+        self.ktab_t = self.koff_t = None
+        if kind == "cells":
+            # cell-minor copy of u, ell, C and L for coalesced per-cell reads
+            parts, offs_t = [], np.full(kmax + 1, -1, dtype=np.int64)
+            pos = 0
+            for k in plan.ks:
+                F = self.factors[k]
+                n = nv * ng
+                u_ = F[:n].reshape(nv, ng).T
+                ell_ = F[n:2 * n].reshape(nv, ng).T
+                L_ = F[2 * n:2 * n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
+                C_ = F[2 * n + nv * ng * ng:2 * n + nv * ng * ng + n].reshape(nv, ng).T
+                t = np.concatenate([u_.ravel(), ell_.ravel(), C_.ravel(), L_.ravel()])
+                offs_t[k] = pos
+                pos += t.shape[0]
+                parts.append(t)
+            self.ktab_t = torch.as_tensor(np.concatenate(parts), device=d)
+            self.koff_t = torch.as_tensor(offs_t, device=d)
         self.max_z = max_z
         self.body_w = fused_body_width(nv, ng) if self.fused else self.kbody
         self.kdim = {k: _round_up(self.body_w + self.nz[k], self.KCHUNK) for k in plan.ks}
@@ -184,6 +225,16 @@ class IonRows:
         b_ptr = resB.data_ptr() + rb * kpad if resB is not None else 0
         rs, lf = rowscale.data_ptr() + 8 * rb, left.data_ptr() + 8 * rb * cwp
         rt, cb = right.data_ptr() + 8 * rb * cwp, cbound.data_ptr() + 16 * rb
+        if self.kind == "cells":
+            _native.check(L.rkb_split_rows_cells(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                                 dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                                 dev.w.data_ptr(), dev.nv, dev.ng, self.ktab.data_ptr(),
+                                                 self.koff.data_ptr(), self.ktab_t.data_ptr(), self.koff_t.data_ptr(),
+                                                 self.max_z, bits, n_mod, moduli_c, a_ptr,
+                                                 b_ptr, kpad, 0, nrows_total, rs, lf, rt, cb, cwp,
+                                                 _native.stream_handle(stream)),
+                          "rkb_split_rows_cells")
+            return
         if self.fused:
             _native.check(L.rkb_split_rows_fused(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
                                                  dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
@@ -207,12 +258,13 @@ class SplitEngine:
     KCHUNK = 128
 
     def __init__(self, dev: IonDevice, bits: int | None = None, tau: float = 1e-3, n_mod: int | None = None,
-                 corr_floor: float | None = None, fused: bool | None = None, materialize: bool = True):
+                 corr_floor: float | None = None, fused: bool | None = None, materialize: bool = True,
+                 rows_kernel: str | None = None):
         _native.require_device()
         self.dev = dev
         plan = dev.plan
         nv, ng = dev.nv, dev.ng
-        self.ion_rows = R = IonRows(dev, tau=tau, fused=fused)
+        self.ion_rows = R = IonRows(dev, tau=tau, fused=fused, rows_kernel=rows_kernel)
         self.factors, self.ktab, self.koff, self.kbody, self.nz = R.factors, R.ktab, R.koff, R.kbody, R.nz
         self.fused, self.max_z, self.body_w, self.kdim, self.zcount = R.fused, R.max_z, R.body_w, R.kdim, R.zcount
         d = dev.Pv.device
@@ -233,7 +285,7 @@ class SplitEngine:
         self.right = torch.empty_like(self.left)
         self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
         # scratch of the two-kernel path: the FP64 rows [X | Z] before rounding
-        self.xwork = None if self.fused else torch.empty((nrows, self.kpad), dtype=torch.float64, device=d)
+        self.xwork = (torch.empty((nrows, self.kpad), dtype=torch.float64, device=d) if R.kind == "two" else None)
         #: skip the FP64 core correction of a block when its bound is below
         #: 2^-(bits+10) of the block's scale (none of the entries can move by
         #: more than that; the split's own error is ~2^-bits of the same scale)
@@ -265,7 +317,7 @@ class SplitEngine:
 
     @property
     def launches_per_step(self) -> int:
-        return 2 if self.fused else 3
+        return 3 if self.ion_rows.kind == "two" else 2
 
     def column_positions(self, k: int) -> np.ndarray:
         """Residue position of every column of the row [X | Z] of multipole k."""
@@ -338,6 +390,7 @@ class SplitEngine:
 
     def info(self) -> dict:
         return {"bits": self.bits, "n_mod": self.n_mod, "moduli": [int(m) for m in self.moduli], "fused": self.fused,
+                "rows_kernel": self.ion_rows.kind,
                 "kpad": self.kpad, "z_columns": {int(k): v for k, v in self.nz.items()},
                 "device_bytes": self.device_bytes(),
                 "tasks": self.n_tasks}

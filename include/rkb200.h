@@ -189,6 +189,22 @@ int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long orb_ld, co
                          long kpad, long row_base, long nrows_total, double *d_rowscale,
                          double *d_left, double *d_right, double *d_cbound, int cwp, void *stream);
 
+/* rkb_split_rows_cells: the rkb_split_rows computation with one block per
+ * row and one thread per cell (5 <= ng <= 11, nv + max_z <= 256 threads,
+ * max_z <= 64), no FP64 workspace; residue columns in natural order
+ * ((m-1)*ng + node, then Z), positions from (nv-1)*ng + nZ up to kpad
+ * written as zeros.  Besides the packed tables (d_ktab/d_koff) it reads a
+ * cell-minor copy of each multipole's factors at d_ktab_t + d_koff_t[k]:
+ * u[ng][nv] | ell[ng][nv] | C[ng][nv] | L[ng][ng][nv] (L[i][node][cell]).
+ * Scales, core vectors and bounds as rkb_split_rows. */
+int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
+                         const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
+                         int nv, int ng, const double *d_ktab, const long *d_koff,
+                         const double *d_ktab_t, const long *d_koff_t, int max_z, int bits,
+                         int n_mod, const int *moduli, signed char *d_resA, signed char *d_resB,
+                         long kpad, long row_base, long nrows_total, double *d_rowscale,
+                         double *d_left, double *d_right, double *d_cbound, int cwp, void *stream);
+
 /* Host-only planning (no device work): the packed factored Green operator of
  * multipole k on the grid r (nv cells x ng nodes, mo/mi the ng x ng partial
  * matrices of atomx numerics/yk.py:65 yk_partial_matrices) with eigenvalue

@@ -42,11 +42,11 @@ def _engine(name, **opts):
     return ion, Pg, Qg, dev, SplitEngine(dev, **opts)
 
 
-@pytest.mark.parametrize("name,fused", [("neon_small", False), ("neon_small", True),
-                                        ("ytterbium_scaleup", False), ("ytterbium_scaleup", True)])
-def test_rows_kernel_matches_cpu_transform(name, fused):
-    ion, Pg, Qg, dev, eng = _engine(name, fused=fused)
-    assert eng.fused == fused
+@pytest.mark.parametrize("name", ["neon_small", "ytterbium_scaleup"])
+@pytest.mark.parametrize("rows_kernel", ["two", "fused", "cells"])
+def test_rows_kernel_matches_cpu_transform(name, rows_kernel):
+    ion, Pg, Qg, dev, eng = _engine(name, rows_kernel=rows_kernel)
+    assert eng.ion_rows.kind == rows_kernel
     eng.rows()
     torch.cuda.synchronize()
     plan = dev.plan
@@ -160,14 +160,14 @@ def _schwarz_err(T, ref_vals, ii, jj):
     return np.abs(T[ii, jj] - ref_vals) / np.sqrt(d[ii] * d[jj])
 
 
-@pytest.mark.parametrize("fused", [False, True])
-def test_split_table_neon_every_entry(fused):
+@pytest.mark.parametrize("rows_kernel", ["two", "fused", "cells"])
+def test_split_table_neon_every_entry(rows_kernel):
     from atomx_b200 import workloads as W
     from atomx_b200.tables import slater_rk_tables
     g = np.load(os.path.join(GOLDEN, "neon_small.npz"))
     ion = W.build_ion(W.neon_small())
-    tab = slater_rk_tables(ion, precision="split", fused=fused)
-    assert tab.info["fused"] == fused
+    tab = slater_rk_tables(ion, precision="split", rows_kernel=rows_kernel)
+    assert tab.info["rows_kernel"] == rows_kernel
     worst = 0.0
     for k in tab.ks:
         T = tab.table(k).cpu().numpy()
