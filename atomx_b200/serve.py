@@ -5,8 +5,8 @@ kappas, and k_max. This is what an SCF or CI client holds when it asks for
 R^k tables. The server runs each request through three stages:
 
 1. host planning, in a worker pool: the pair/row plan and, for the split
-   engine, the factored Green operators of the grid (cached by grid
-   content);
+   engine, the factored Green operators of the grid and their packed host
+   tables (cached by grid content);
 2. admission: requests leave the ready queue in arrival order while their
    device footprint fits the HBM budget beside the requests already on the
    GPU, and while a stream slot is free. The footprint is the coefficients,
@@ -40,7 +40,7 @@ import numpy as np
 import torch
 
 from .plan import make_plan
-from .split import factors_for_grid
+from .split import host_tables
 from .split_plan import moduli_needed
 from .tables import upload_ion
 
@@ -141,8 +141,8 @@ class SlaterServer:
     def _plan(self, req: Request) -> Request:
         req.plan = make_plan(req.ion.kappa, req.k_max)
         if self.precision == "split":
-            factors_for_grid(np.asarray(req.ion.bsp["gr"], dtype=np.float64).reshape(-1), req.ion.bsp["gr"].shape[1],
-                             req.plan.ks)
+            host_tables(np.asarray(req.ion.bsp["gr"], dtype=np.float64).reshape(-1), req.ion.bsp["gr"].shape[1],
+                        req.plan.ks)
         req.footprint = footprint_bytes(req.ion, req.plan, self.precision)
         req.entries = req.plan.ordered_entries
         return req

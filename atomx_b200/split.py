@@ -30,7 +30,7 @@ from .split_plan import (bits_for_moduli, concat_tables, crt_constants, green_fa
                          table_z_count)
 from .tables import IonDevice, tile_tasks
 
-__all__ = ["SplitEngine", "IonRows", "factors_for_grid", "choose_width", "DEFAULT_BITS"]
+__all__ = ["SplitEngine", "IonRows", "factors_for_grid", "host_tables", "choose_width", "DEFAULT_BITS"]
 
 #: the split is at least this wide by default; ``bits=None`` then widens it to
 #: what the same number of CRT moduli still holds exactly (free accuracy)
@@ -78,6 +78,49 @@ def factors_for_grid(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict
                     _factor_cache.clear()
                 _factor_cache[key] = F
         out[int(k)] = F
+    return out
+
+
+_host_cache: dict = {}
+
+
+def host_tables(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
+    """Host-side tables of a grid and multipole set, cached: the packed factor
+    tables concatenated (``flat``, ``koff``), their Z counts, and the
+    cell-minor copy the cell row kernel reads (``flat_t``, ``koff_t``).
+    Pure host work, so a serving planner can prepare it off the launch path."""
+    r_flat = np.ascontiguousarray(r_flat, dtype=np.float64)
+    ks = tuple(int(k) for k in ks)
+    key = (hashlib.blake2b(r_flat.tobytes(), digest_size=16).hexdigest(), ng, tau, ks)
+    with _factor_lock:
+        hit = _host_cache.get(key)
+    if hit is not None:
+        return hit
+    factors = factors_for_grid(r_flat, ng, ks, tau=tau)
+    nv = r_flat.shape[0] // ng
+    n = nv * ng
+    kmax = max(ks)
+    flat, offs = concat_tables([factors[k] for k in ks])
+    koff = np.full(kmax + 1, -1, dtype=np.int64)
+    koff_t = np.full(kmax + 1, -1, dtype=np.int64)
+    parts, pos = [], 0
+    for i, k in enumerate(ks):
+        koff[k] = offs[i]
+        F = factors[k]
+        u_ = F[:n].reshape(nv, ng).T
+        ell_ = F[n:2 * n].reshape(nv, ng).T
+        L_ = F[2 * n:2 * n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
+        C_ = F[2 * n + nv * ng * ng:2 * n + nv * ng * ng + n].reshape(nv, ng).T
+        t = np.concatenate([u_.ravel(), ell_.ravel(), C_.ravel(), L_.ravel()])
+        koff_t[k] = pos
+        pos += t.shape[0]
+        parts.append(t)
+    out = {"factors": factors, "flat": flat, "koff": koff, "flat_t": np.concatenate(parts), "koff_t": koff_t,
+           "nz": {k: table_z_count(factors[k], nv, ng) for k in ks}}
+    with _factor_lock:
+        if len(_host_cache) > 256:
+            _host_cache.clear()
+        _host_cache[key] = out
     return out
 
 
@@ -135,17 +178,14 @@ class IonRows:
         r_host = dev.extra.get("r_host")
         if r_host is None:
             r_host = dev.r.detach().cpu().numpy()
-        self.factors = factors_for_grid(r_host, ng, plan.ks, tau=tau)
+        H = host_tables(r_host, ng, plan.ks, tau=tau)
+        self.factors = H["factors"]
         kmax = max(plan.ks)
-        flat, offs = concat_tables([self.factors[k] for k in plan.ks])
-        koff = np.full(kmax + 1, -1, dtype=np.int64)
-        for i, k in enumerate(plan.ks):
-            koff[k] = offs[i]
         d = dev.Pv.device
-        self.ktab = torch.as_tensor(flat, device=d)
-        self.koff = torch.as_tensor(koff, device=d)
+        self.ktab = torch.as_tensor(H["flat"], device=d)
+        self.koff = torch.as_tensor(H["koff"], device=d)
         self.kbody = (nv - 1) * ng
-        self.nz = {k: table_z_count(self.factors[k], nv, ng) for k in plan.ks}
+        self.nz = dict(H["nz"])
         max_z = max(self.nz.values())
         fits = fused_fits(nv, ng, max_z)
         if fused and not fits:
@@ -178,23 +218,9 @@ class IonRows:
         self.kind = kind
         self.fused = kind == "fused"
         self.ktab_t = self.koff_t = None
-        if kind == "cells":
-            # cell-minor copy of u, ell, C and L for coalesced per-cell reads
-            parts, offs_t = [], np.full(kmax + 1, -1, dtype=np.int64)
-            pos = 0
-            for k in plan.ks:
-                F = self.factors[k]
-                n = nv * ng
-                u_ = F[:n].reshape(nv, ng).T
-                ell_ = F[n:2 * n].reshape(nv, ng).T
-                L_ = F[2 * n:2 * n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
-                C_ = F[2 * n + nv * ng * ng:2 * n + nv * ng * ng + n].reshape(nv, ng).T
-                t = np.concatenate([u_.ravel(), ell_.ravel(), C_.ravel(), L_.ravel()])
-                offs_t[k] = pos
-                pos += t.shape[0]
-                parts.append(t)
-            self.ktab_t = torch.as_tensor(np.concatenate(parts), device=d)
-            self.koff_t = torch.as_tensor(offs_t, device=d)
+        if kind == "cells":  # cell-minor copy of u, ell, C and L for coalesced per-cell reads
+            self.ktab_t = torch.as_tensor(H["flat_t"], device=d)
+            self.koff_t = torch.as_tensor(H["koff_t"], device=d)
         self.max_z = max_z
         self.body_w = fused_body_width(nv, ng) if self.fused else self.kbody
         self.kdim = {k: _round_up(self.body_w + self.nz[k], self.KCHUNK) for k in plan.ks}
