@@ -674,12 +674,12 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
 // K3s — tcgen05 INT8 residue SYRK with CRT epilogue
 // =========================================================================
 constexpr int BM = 128, BN = 128, BKB = 128;  // tile rows, tile cols, K bytes per stage
-constexpr int STAGES = 4;
+constexpr int STAGES = 5;
 constexpr int STAGE_BYTES = (BM + BN) * BKB;  // 32 KB
 constexpr int EPI_WARPS = 16;                 // 4 TMEM lane quarters x 4 column groups
 constexpr int EPI_COLS = BN / (EPI_WARPS / 4);  // columns per epilogue thread
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr int STG_LD = 17;  // doubles per staged row (16 + pad)
+constexpr int STG_LD = 9;   // doubles per staged row (8 + pad)
 constexpr size_t SMEM_BYTES = 1024 /*align slack*/ + (size_t)STAGES * STAGE_BYTES +
                               (size_t)EPI_WARPS * 32 * STG_LD * sizeof(double) + 256 /*barriers*/;
 constexpr long long WAIT_LIMIT = 4000000000LL;  // clock64 ticks (~2 s)
@@ -1035,16 +1035,16 @@ __global__ void __launch_bounds__(THREADS, 1)
                         if (!isfinite(v)) atomicExch(status, (int)RKB_ENONFINITE);
                         if (mirror) R[b * n + a] = v;  // lanes hold consecutive a: coalesced
                     }
-                    stg[lane * STG_LD + (c & 1) * FC + j] = v;
+                    stg[lane * STG_LD + j] = v;
                 }
-                if (c & 1) {
-                    // direct tile row segment of 16 columns through shared memory (coalesced rows)
+                {
+                    // direct tile row segments of 8 columns through shared memory (coalesced rows)
                     __syncwarp();
                     const long a0 = (long)ti * BM + quarter * 32;
-                    const long bc = b0 + (c - 1) * FC;
+                    const long bc = b0 + c * FC;
 #pragma unroll 4
-                    for (int rr = 0; rr < 32; rr += 2) {
-                        const int row = rr + (lane >> 4), col = lane & 15;
+                    for (int rr = 0; rr < 32; rr += 4) {
+                        const int row = rr + (lane >> 3), col = lane & 7;
                         const long aa = a0 + row, bb = bc + col;
                         if (aa < n && bb < n) R[aa * n + bb] = stg[row * STG_LD + col];
                     }
