@@ -29,6 +29,9 @@ _SIGNATURES = {
     "rkb_pair_density": [_vp, _vp, _l, _vp, _l, _l, _vp, _l, _vp],
     "rkb_weighted_dots": [_vp, _l, _vp, _l, _vp, _l, _vp, _vp, _l, _vp, _vp],
     "rkb_slater_direct": [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp],
+    "rkb_grid_yk_rows": [_vp, _l, _vp, _l, _vp, _l, _vp, _vp, _vp, _l, _vp, _l, _l, _vp, _l, _vp],
+    "rkb_grid_pair_dot_batch": [_vp, _vp, _vp, _vp, _l, _vp, _vp, _vp, _vp, _l, _vp, _l, _vp, _vp, _vp, _l, _vp,
+                                _vp, _vp, _l, _vp, _l, _l, _vp, _vp, _l, _vp],
     "rkb_table_rows_fp64": [_vp, _vp, _l, _vp, _vp, _vp, _l, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _l, _vp],
     "rkb_table_contract_fp64": [_vp, _vp, _l, _l, _vp, _vp, _vp, _vp, _l, _vp, _vp],
     "rkb_table_contract_fp64_groups": [_vp, _vp, _l, _l, _vp, _vp, _vp, _vp, _vp, _l, _vp, _vp],

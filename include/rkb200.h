@@ -91,6 +91,40 @@ int rkb_slater_direct(const double *d_rho13, const double *d_rho24, const double
                       const double *d_inner, double *d_out, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Arbitrary-grid trapezoid Y^k (atomx numerics/quadrature.py).
+ *
+ * Tables for a grid r[n] and ranks 0..K (atomx quadrature.py:190-231
+ * _coulomb_tables): d_RK and d_inverse are (K+1) x n (block-scaled r^k and
+ * r^-(k+1)), d_cuts[ncuts] the frame starts (d_cuts[ncuts-1] = n) and
+ * d_transfers (K+1) x ntr (ntr >= ncuts-2) the frame-change factors.
+ *
+ * rkb_grid_yk_rows mirrors quadrature.py:234 yk_on_grid per row: row m
+ * reads d_rho + m*rho_ld and rank d_rows_k[m], and writes Y^k at points
+ * 0..i_cut of d_y + m*y_ld.
+ *
+ * rkb_grid_pair_dot_batch mirrors quadrature.py:282 yk_pair_dot_batch_on_grid:
+ * row m forms rho = PA[a]PB[b] + QA[a]QB[b] (a = d_rows_a[m], b =
+ * d_rows_b[m], rows of stride ld), takes Y^k (k = d_rows_k[m]) on points
+ * 0..i_cut and, for each consumer slot s in [d_cons_ptr[m], d_cons_ptr[m+1]),
+ * writes d_val[s] = sum_i W[d_cons_rho[s]][i] Y_i (W rows of stride w_ld).
+ * Rows with d_rows_ok[m] == 0 leave their slots untouched (zero them first).
+ * d_work: work_rows x n doubles of scratch (one row per concurrent CTA).
+ * ------------------------------------------------------------------------- */
+int rkb_grid_yk_rows(const double *d_rho, long rho_ld, const long *d_rows_k, long nrows,
+                     const double *d_r, long n, const double *d_RK, const double *d_inverse,
+                     const long *d_cuts, long ncuts, const double *d_transfers, long ntr, long i_cut,
+                     double *d_y, long y_ld, void *stream);
+
+int rkb_grid_pair_dot_batch(const double *d_PA, const double *d_QA, const double *d_PB,
+                            const double *d_QB, long ld, const long *d_rows_a, const long *d_rows_b,
+                            const long *d_rows_k, const unsigned char *d_rows_ok, long nrows,
+                            const double *d_W, long w_ld, const long *d_cons_ptr,
+                            const long *d_cons_rho, const double *d_r, long n, const double *d_RK,
+                            const double *d_inverse, const long *d_cuts, long ncuts,
+                            const double *d_transfers, long ntr, long i_cut, double *d_val,
+                            double *d_work, long work_rows, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Plain FP64 table engine (all arithmetic in FP64).
  *
  * rkb_table_rows_fp64: for each row q of a plan (pair d_row_pair[q], multipole

@@ -14,6 +14,9 @@ its project root) in plain numpy or calls the C restatement in
 * ``slater_rk_poisson``     <- src/atomx/numerics/bspline/slater.py:118-130
 * ``slater_rk_direct``      <- src/atomx/numerics/bspline/slater.py:51-115
 * ``dot_entries``           <- slater.py:130, one dot per ordered table entry
+* ``coulomb_tables``        <- src/atomx/numerics/quadrature.py:190-231 (numpy)
+* ``yk_on_grid`` / ``grid_slater_rk`` / ``yk_pair_dot_batch_on_grid``
+                            <- quadrature.py:234-404 (C, bit-faithful)
 
 Parity of the oracle itself is pinned against vectors generated by running
 the reference (tests/golden/make_golden.py) and against closed forms.
@@ -199,3 +202,114 @@ def slater_rk_direct(rho13, rho24, gr, grw, k):
     dens = fo[:, :, None] * gi + go[:, :, None] * fi
     diag = float(np.sum(dens * kj * wt[None, :, None] * wt[None, None, :]))
     return off + diag
+
+
+# --------------------------------------------------------------------------
+# Arbitrary-grid trapezoid Y^k (atomx src/atomx/numerics/quadrature.py)
+# --------------------------------------------------------------------------
+def coulomb_tables(r, k_max):
+    """Block-scaled power tables (quadrature.py:190-231, ``_coulomb_tables``).
+
+    Within a block x = r / r_anchor and (k_max + 1) log x <= 128, so the powers
+    stay far from overflow; moving between blocks multiplies carried moments
+    by (smaller anchor / larger anchor)^k <= 1.  Same numpy operations as the
+    reference; returns (rk, inverse, cuts, transfers).
+    """
+    if isinstance(k_max, (bool, np.bool_)) or int(k_max) != k_max or k_max < 0:
+        raise ValueError('Coulomb multipole rank must be a nonnegative integer')
+    r = np.asarray(r, dtype=float)
+    if (r.ndim != 1 or not r.size or not np.isfinite(r).all()
+            or np.any(r <= 0) or np.any(np.diff(r) <= 0)):
+        raise ValueError('Coulomb grid must be finite, positive and strictly increasing')
+    logs, cuts = np.log(r), [0]
+    span = 128. / (k_max + 1)
+    while cuts[-1] < len(r):
+        stop = int(np.searchsorted(logs, logs[cuts[-1]] + span, side='right'))
+        cuts.append(max(cuts[-1] + 1, stop))
+    cuts = np.asarray(cuts, dtype=np.int64)
+    anchors = r[cuts[:-1]]
+    rk = np.empty((k_max + 1, len(r)))
+    inverse = np.empty_like(rk)
+    orders = np.arange(k_max + 1)[:, None]
+    for block in range(len(anchors)):
+        lo, hi = cuts[block:block + 2]
+        x = r[lo:hi] / anchors[block]
+        rk[:, lo:hi] = x[None, :] ** orders
+        inverse[:, lo:hi] = x[None, :] ** (-orders - 1) / anchors[block]
+    transfers = ((anchors[:-1] / anchors[1:])[None, :] ** np.arange(k_max + 1)[:, None])
+    return rk, inverse, cuts, transfers
+
+
+def _grid_lib():
+    lib = _lib()
+    if not hasattr(lib, "_grid_bound"):
+        lib.oracle_grid_yk_rho.argtypes = [_dptr, _dptr, ctypes.c_long, _dptr, _dptr, _lptr, ctypes.c_long, _dptr,
+                                           ctypes.c_long, _dptr]
+        lib.oracle_grid_yk_rho.restype = None
+        lib.oracle_grid_pair_yk.argtypes = [_dptr, _dptr, _dptr, _dptr, _dptr, ctypes.c_long, _dptr, _dptr, _lptr,
+                                            ctypes.c_long, _dptr, ctypes.c_long, _dptr]
+        lib.oracle_grid_pair_yk.restype = None
+        lib.oracle_grid_slater_rk.argtypes = [_dptr] * 9 + [ctypes.c_long, _dptr, _dptr, _lptr, ctypes.c_long,
+                                                            _dptr, _dptr]
+        lib.oracle_grid_slater_rk.restype = ctypes.c_double
+        lib.oracle_grid_pair_dot_batch.argtypes = [_dptr, _dptr, _dptr, _dptr, ctypes.c_long, _lptr, _lptr, _lptr,
+                                                   ctypes.POINTER(ctypes.c_ubyte), ctypes.c_long, _dptr,
+                                                   ctypes.c_long, _lptr, _lptr, _dptr, ctypes.c_long, _dptr, _dptr,
+                                                   _lptr, ctypes.c_long, _dptr, ctypes.c_long, ctypes.c_long, _dptr,
+                                                   ctypes.c_int]
+        lib.oracle_grid_pair_dot_batch.restype = None
+        lib._grid_bound = True
+    return lib
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def yk_on_grid(rho, r, k, i_cut=None):
+    """quadrature.py:234-244: trapezoidal Green action on a radial density."""
+    r = _c(r)
+    rk, inverse, cuts, transfers = coulomb_tables(r, k)
+    n = r.shape[0]
+    ic = n - 1 if i_cut is None else min(int(i_cut), n - 1)
+    y = np.empty(ic + 1 if ic + 1 > n else n)
+    rk_k, inv_k, tr_k = _c(rk[k]), _c(inverse[k]), _c(transfers[k])
+    _grid_lib().oracle_grid_yk_rho(_p(_c(rho)), _p(r), n, _p(rk_k), _p(inv_k), _p(_c(cuts, np.int64), _lptr),
+                                   cuts.shape[0], _p(tr_k), ic, _p(y))
+    return y[:ic + 1].copy()
+
+
+def grid_slater_rk(P_a, Q_a, P_b, Q_b, P_c, Q_c, P_d, Q_d, r_grid, k):
+    """quadrature.py:394-404: R^k(a,b,c,d) = Int rho_ac Y^k[rho_bd] dr."""
+    r = _c(r_grid)
+    rk, inverse, cuts, transfers = coulomb_tables(r, k)
+    work = np.empty(r.shape[0])
+    args = [_p(_c(x)) for x in (P_a, Q_a, P_b, Q_b, P_c, Q_c, P_d, Q_d)]
+    return float(_grid_lib().oracle_grid_slater_rk(*args, _p(r), r.shape[0], _p(_c(rk[k])), _p(_c(inverse[k])),
+                                                   _p(_c(cuts, np.int64), _lptr), cuts.shape[0],
+                                                   _p(_c(transfers[k])), _p(work)))
+
+
+def yk_pair_dot_batch_on_grid(PA, QA, PB, QB, rows_a, rows_b, rows_k, rows_ok, RhoA, cons_ptr, cons_rho, r,
+                              i_cut=None, threads: int = 0):
+    """quadrature.py:282-310: batched Int rho_w Y^k[rho_ab] dr with CSR consumers."""
+    r = _c(r)
+    n = r.shape[0]
+    ic = n - 1 if i_cut is None else min(int(i_cut), n - 1)
+    cons_ptr = _c(cons_ptr, np.int64)
+    val = np.zeros(cons_ptr[-1] if cons_ptr.shape[0] else 0)
+    rows_a = _c(rows_a, np.int64)
+    if rows_a.shape[0] == 0:
+        return val
+    rows_k = _c(rows_k, np.int64)
+    RK, inverse, cuts, transfers = coulomb_tables(r, int(rows_k.max()))
+    PA, QA, PB, QB = (_c(x) for x in (PA, QA, PB, QB))
+    RhoA = _c(RhoA)
+    ok = _c(rows_ok, np.uint8)
+    _grid_lib().oracle_grid_pair_dot_batch(
+        _p(PA), _p(QA), _p(PB), _p(QB), PA.shape[1], _p(rows_a, _lptr), _p(_c(rows_b, np.int64), _lptr),
+        _p(rows_k, _lptr), ok.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), rows_a.shape[0], _p(RhoA),
+        RhoA.shape[1], _p(cons_ptr, _lptr), _p(_c(cons_rho, np.int64), _lptr), _p(r), n, _p(_c(RK)),
+        _p(_c(inverse)), _p(_c(cuts, np.int64), _lptr), cuts.shape[0], _p(_c(transfers)), transfers.shape[1], ic,
+        _p(val), threads)
+    return val

@@ -20,6 +20,9 @@
  *       dot per ordered table entry, as the reference evaluates it per
  *       integral.
  *
+ *   oracle_grid_*     <- src/atomx/numerics/quadrature.py:247-391 (trapezoid Y^k
+ *       on arbitrary grids; see the section at the end of this file).
+ *
  * Parity of this oracle is pinned by tests against golden vectors produced by
  * running the reference itself (tests/golden/make_golden.py).
  */
@@ -165,4 +168,141 @@ void oracle_dot_table(const double *g, const double *y, long n,
 {
     struct dot_ctx c = {g, y, ia, ib, out, n};
     parallel_for(dot_range, &c, nent, threads);
+}
+
+/* ------------------------------------------------------------------------
+ * Arbitrary-grid trapezoid Y^k (atomx src/atomx/numerics/quadrature.py).
+ *
+ * oracle_grid_yk_rho    <- quadrature.py:247-279 (_yk_kernel_rho)
+ * oracle_grid_pair_yk   <- quadrature.py:313-352 (_pair_yk: fused density)
+ * oracle_grid_slater_rk <- quadrature.py:375-391 (_slater_rk_kernel)
+ * oracle_grid_pair_dot_batch <- quadrature.py:282-310, 355-372
+ *
+ * The tables rk / inverse (block-scaled powers), the block starts `cuts`
+ * and the frame transfers come from the numpy restatement of
+ * _coulomb_tables (quadrature.py:190-231) in oracle.py.  The scans run in the
+ * reference's order: inward cumulative trapezoids from the last node, the
+ * carry rescaled by the transfer at each block change, then outward with
+ * y_i = inner_i * inverse_i + rk_i * y_i.  Each expression keeps the
+ * reference's operation order.  Pinned results: bit-identical for the batch
+ * and Y^k functions; for grid_slater_rk with nonzero small components the
+ * reference (one Numba function with the scan inlined) rounds a few
+ * multiply-adds as fused operations, and the values agree to ~1e-16.
+ * ------------------------------------------------------------------------ */
+#define GRID_SCAN(DENS)                                                        \
+    do {                                                                       \
+        double acc = 0.0, prev = (DENS(n - 1)) * inverse[n - 1];               \
+        if (i_cut == n - 1) y[n - 1] = 0.0;                                    \
+        for (long block = ncuts - 2; block >= 0; --block) {                    \
+            if (block < ncuts - 2) {                                           \
+                acc *= transfer[block];                                        \
+                prev *= transfer[block];                                       \
+            }                                                                  \
+            long top = cuts[block + 1] - 1 < n - 2 ? cuts[block + 1] - 1 : n - 2; \
+            for (long i = top; i >= cuts[block]; --i) {                        \
+                double b = (DENS(i)) * inverse[i];                             \
+                acc += .5 * (b + prev) * (r[i + 1] - r[i]);                    \
+                if (i <= i_cut) y[i] = acc;                                    \
+                prev = b;                                                      \
+            }                                                                  \
+        }                                                                      \
+        double inner = 0.0;                                                    \
+        prev = (DENS(0)) * rk[0];                                              \
+        y[0] *= rk[0];                                                         \
+        for (long block = 0; block < ncuts - 1; ++block) {                     \
+            if (cuts[block] > i_cut) break;                                    \
+            if (block) {                                                       \
+                inner *= transfer[block - 1];                                  \
+                prev *= transfer[block - 1];                                   \
+            }                                                                  \
+            long lo = cuts[block] > 1 ? cuts[block] : 1;                       \
+            long hi = cuts[block + 1] < i_cut + 1 ? cuts[block + 1] : i_cut + 1; \
+            for (long i = lo; i < hi; ++i) {                                   \
+                double a = (DENS(i)) * rk[i];                                  \
+                inner += .5 * (a + prev) * (r[i] - r[i - 1]);                  \
+                y[i] = (inner * inverse[i] + rk[i] * y[i]);                    \
+                prev = a;                                                      \
+            }                                                                  \
+        }                                                                      \
+    } while (0)
+
+void oracle_grid_yk_rho(const double *rho, const double *r, long n, const double *rk, const double *inverse,
+                        const long *cuts, long ncuts, const double *transfer, long i_cut, double *y)
+{
+#define RHO_AT(i) rho[(i)]
+    GRID_SCAN(RHO_AT);
+#undef RHO_AT
+}
+
+void oracle_grid_pair_yk(const double *Pa, const double *Qa, const double *Pb, const double *Qb, const double *r,
+                         long n, const double *rk, const double *inverse, const long *cuts, long ncuts,
+                         const double *transfer, long i_cut, double *y)
+{
+#define PAIR_AT(i) (Pa[(i)] * Pb[(i)] + Qa[(i)] * Qb[(i)])
+    GRID_SCAN(PAIR_AT);
+#undef PAIR_AT
+}
+
+double oracle_grid_slater_rk(const double *Pa, const double *Qa, const double *Pb, const double *Qb,
+                             const double *Pc, const double *Qc, const double *Pd, const double *Qd,
+                             const double *r, long n, const double *rk, const double *inverse, const long *cuts,
+                             long ncuts, const double *transfer, double *work)
+{
+    long i_cut = 0;
+    for (long i = n - 1; i >= 0; --i) {
+        if (Pa[i] * Pc[i] + Qa[i] * Qc[i] != 0.0) {
+            i_cut = i + 1 < n - 1 ? i + 1 : n - 1;
+            break;
+        }
+    }
+    oracle_grid_pair_yk(Pb, Qb, Pd, Qd, r, n, rk, inverse, cuts, ncuts, transfer, i_cut, work);
+    double prev = (Pa[0] * Pc[0] + Qa[0] * Qc[0]) * work[0];
+    double total = 0.0;
+    for (long i = 1; i <= i_cut; ++i) {
+        double g = (Pa[i] * Pc[i] + Qa[i] * Qc[i]) * work[i];
+        total += .5 * (g + prev) * (r[i] - r[i - 1]);
+        prev = g;
+    }
+    return total;
+}
+
+struct grid_batch_ctx {
+    const double *PA, *QA, *PB, *QB; long ld;
+    const long *rows_a, *rows_b, *rows_k; const unsigned char *rows_ok;
+    const double *RhoA; long rho_ld; const long *cons_ptr, *cons_rho;
+    const double *r; long n; const double *RK, *inverse; const long *cuts; long ncuts;
+    const double *transfers; long ntr; long i_cut; double *val;
+};
+
+static void grid_batch_range(void *vctx, long lo, long hi)
+{
+    struct grid_batch_ctx *c = (struct grid_batch_ctx *)vctx;
+    double *y = (double *)malloc(sizeof(double) * (size_t)(c->i_cut + 1 > c->n ? c->i_cut + 1 : c->n));
+    for (long m = lo; m < hi; ++m) {
+        long s0 = c->cons_ptr[m], s1 = c->cons_ptr[m + 1];
+        if (!c->rows_ok[m] || s0 == s1) continue;
+        long ia = c->rows_a[m], ib = c->rows_b[m], k = c->rows_k[m];
+        oracle_grid_pair_yk(c->PA + ia * c->ld, c->QA + ia * c->ld, c->PB + ib * c->ld, c->QB + ib * c->ld, c->r,
+                            c->n, c->RK + k * c->n, c->inverse + k * c->n, c->cuts, c->ncuts,
+                            c->transfers + k * c->ntr, c->i_cut, y);
+        for (long s = s0; s < s1; ++s) {
+            double total = 0.0;
+            const double *w = c->RhoA + c->cons_rho[s] * c->rho_ld;
+            for (long i = 0; i <= c->i_cut; ++i) total += w[i] * y[i];
+            c->val[s] = total;
+        }
+    }
+    free(y);
+}
+
+void oracle_grid_pair_dot_batch(const double *PA, const double *QA, const double *PB, const double *QB, long ld,
+                                const long *rows_a, const long *rows_b, const long *rows_k,
+                                const unsigned char *rows_ok, long nrows, const double *RhoA, long rho_ld,
+                                const long *cons_ptr, const long *cons_rho, const double *r, long n,
+                                const double *RK, const double *inverse, const long *cuts, long ncuts,
+                                const double *transfers, long ntr, long i_cut, double *val, int threads)
+{
+    struct grid_batch_ctx ctx = {PA, QA, PB, QB, ld, rows_a, rows_b, rows_k, rows_ok, RhoA, rho_ld, cons_ptr,
+                                 cons_rho, r, n, RK, inverse, cuts, ncuts, transfers, ntr, i_cut, val};
+    parallel_for(grid_batch_range, &ctx, nrows, threads);
 }

@@ -26,6 +26,12 @@ atomx.  What each file holds:
 * hydrogenic.npz         atomx physics grid (ks=9, Z=1, r_max=50): nodes and
                          weights, atomx R^k for rho = 4 r^2 e^{-2r} (k=0..2)
                          and rho = e^{-r} (k=0..3) with 40-digit mpmath values.
+* grid_quadrature.npz    atomx arbitrary-grid trapezoid Y^k (quadrature.py):
+                         yk_on_grid / grid_slater_rk on a 1e-9..100 grid for
+                         ranks up to 256, yk_pair_dot_batch_on_grid on the
+                         reference's batch geometry and on a make_fine_grid
+                         grid with seeded waves, and the endpoint cases.
+                         (``--only grid`` writes just this file.)
 """
 from __future__ import annotations
 
@@ -39,12 +45,82 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 
 
+def grid_quadrature():
+    """Golden vectors of atomx's arbitrary-grid trapezoid Y^k
+    (numerics/quadrature.py): yk_on_grid, grid_slater_rk and
+    yk_pair_dot_batch_on_grid on the reference's own test geometries plus a
+    composite fine grid (make_fine_grid) with seeded random waves."""
+    from atomx.numerics.quadrature import (grid_slater_rk, make_fine_grid, yk_on_grid,
+                                           yk_pair_dot_batch_on_grid)
+    out = {}
+    # A: wide dynamic range, ranks up to 256
+    r = np.geomspace(1e-9, 100.0, 193)
+    rho = np.sin(3 * np.log(r)) * np.exp(-r / 12)
+    other = np.cos(np.log(r)) * np.exp(-r / 9)
+    ones, zeros = np.ones_like(r), np.zeros_like(r)
+    ranks = np.array([0, 1, 12, 32, 64, 128, 256])
+    out["a_r"], out["a_rho"], out["a_other"], out["a_ranks"] = r, rho, other, ranks
+    out["a_yk"] = np.array([yk_on_grid(rho, r, int(k)) for k in ranks])
+    out["a_yk_cut"] = np.array([yk_on_grid(rho, r, int(k), i_cut=97) for k in ranks])
+    out["a_slater"] = np.array([grid_slater_rk(other, zeros, rho, zeros, ones, zeros, ones, zeros, r, int(k))
+                                for k in ranks])
+    # B: the batch geometry with invalid rows, empty and repeated consumers
+    rng = np.random.default_rng(8217)
+    rb = np.geomspace(.013, 9., 81)
+    pa, qa, pb, qb = [rng.normal(size=(4, len(rb))) * np.exp(-rb / 4) for _ in range(4)]
+    a, b = np.array([0, 2, 1, 3]), np.array([1, 0, 2, 0])
+    rks, valid = np.array([0, 1, 3, 2]), np.array([True, True, False, True])
+    ptr, cons = np.array([0, 2, 2, 5, 6]), np.array([0, 2, 1, 0, 3, 1])
+    for cut in (0, 41, 80):
+        outer = rng.normal(size=(4, cut + 1))
+        out[f"b_outer{cut}"] = outer
+        out[f"b_val{cut}"] = yk_pair_dot_batch_on_grid(pa, qa, pb, qb, a, b, rks, valid, outer, ptr, cons, rb,
+                                                       i_cut=cut)
+    out.update(b_r=rb, b_pa=pa, b_qa=qa, b_pb=pb, b_qb=qb, b_a=a, b_b=b, b_k=rks, b_ok=valid, b_ptr=ptr,
+               b_cons=cons)
+    # C: composite fine grid, seeded waves, many rows and consumers
+    rf = np.asarray(make_fine_grid(30.0, 2.0, z_inner=20.0), dtype=float)
+    rng = np.random.default_rng(4411)
+    nw = 6
+    env = np.exp(-rf / 6.0)
+    P = rng.normal(size=(nw, rf.shape[0])) * env
+    Q = 0.01 * rng.normal(size=(nw, rf.shape[0])) * env
+    nrow = 24
+    ra, rbb = rng.integers(0, nw, nrow), rng.integers(0, nw, nrow)
+    rk_ = rng.integers(0, 9, nrow)
+    ok = rng.random(nrow) > 0.1
+    counts = rng.integers(0, 4, nrow)
+    cptr = np.concatenate([[0], np.cumsum(counts)])
+    ccons = rng.integers(0, 5, cptr[-1])
+    cut = int(rf.shape[0] * 0.8)
+    weights = rng.normal(size=(5, cut + 1)) * np.exp(-rf[:cut + 1] / 5.0)
+    out.update(c_r=rf, c_P=P, c_Q=Q, c_a=ra, c_b=rbb, c_k=rk_, c_ok=ok, c_ptr=cptr, c_cons=ccons, c_w=weights,
+               c_cut=np.array(cut))
+    out["c_val"] = yk_pair_dot_batch_on_grid(P, Q, P, Q, ra, rbb, rk_, ok, weights, cptr, ccons, rf, i_cut=cut)
+    out["c_slater"] = np.array([grid_slater_rk(P[0], Q[0], P[1], Q[1], P[2], Q[2], P[3], Q[3], rf, k)
+                                for k in (0, 1, 4)])
+    # D: endpoint rules (support cut with a half interval; a tiny far tail)
+    r4 = np.array([0.1, 0.4, 1.0, 2.0])
+    a4, b4, z4 = np.array([1.0, 2.0, 0.0, 0.0]), np.ones(4), np.zeros(4)
+    r3 = np.array([1e-7, 1.0, 1e20])
+    a3, b3, z3 = np.array([1.0, 1e-20, 1e-20]), np.ones(3), np.zeros(3)
+    out["d_cut"] = np.array(grid_slater_rk(a4, z4, b4, z4, b4, z4, b4, z4, r4, 0))
+    out["d_tail"] = np.array(grid_slater_rk(a3, z3, b3, z3, b3, z3, b3, z3, r3, 0))
+    np.savez_compressed(os.path.join(HERE, "grid_quadrature.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--atomx-src", required=True)
+    ap.add_argument("--only", choices=["grid"], default=None,
+                    help="write only one fixture family (the others are left as they are)")
     args = ap.parse_args()
     sys.path.insert(0, args.atomx_src)
     sys.path.insert(0, REPO)
+    if args.only == "grid":
+        grid_quadrature()
+        print("golden grid fixtures written to", HERE)
+        return
 
     from atomx.numerics.bspline.basis import prepare_bspline_data as ref_prepare
     from atomx.numerics.bspline.dirac_assembly import build_dirac_matrices, solve_dirac
