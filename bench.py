@@ -378,6 +378,8 @@ def run_gpu(args):
     line.update(extra)
     if args.serve > 0 and engine == "split":
         line["serve"] = serve_leg(args)
+    if not args.no_grid and engine == "split":
+        line["grid_yk"] = grid_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
@@ -470,6 +472,76 @@ def serve_leg(args) -> dict:
     return out
 
 
+def grid_leg(rows: int = 4000, n: int = 20000, reps: int = 5) -> dict:
+    """Arbitrary-grid trapezoid Y^k batch (atomx quadrature.yk_pair_dot_batch_on_grid):
+    seeded waves on a geometric grid of n points, `rows` pair rows with ranks
+    0..16 and two consumers each, i_cut = n - 1.  Device time per batch (CUDA
+    events, inputs resident), against the oracle port of the reference's
+    serial kernel on a bounded sample of rows on the host cores."""
+    import torch
+
+    from atomx_b200 import _native
+    from atomx_b200.quadrature import GridTables
+    from oracle import oracle
+    rng = np.random.default_rng(77)
+    r = np.geomspace(1e-4, 80.0, n)
+    env = np.exp(-r / 10.0)
+    nw = 32
+    P = rng.normal(size=(nw, n)) * env
+    Q = 0.02 * rng.normal(size=(nw, n)) * env
+    a, b = rng.integers(0, nw, rows), rng.integers(0, nw, rows)
+    ks = rng.integers(0, 17, rows)
+    ok = np.ones(rows, dtype=bool)
+    ptr = np.arange(0, 2 * rows + 1, 2)
+    cons = rng.integers(0, 8, 2 * rows)
+    W = rng.normal(size=(8, n)) * env
+    dev = torch.device("cuda")
+    tab = GridTables.get(r, 16, dev)
+    d = {k_: torch.as_tensor(v, device=dev) for k_, v in
+         dict(P=P, Q=Q, a=a, b=b, k=ks, ok=ok.astype(np.uint8), ptr=ptr, cons=cons, W=W).items()}
+    val = torch.zeros(2 * rows, dtype=torch.float64, device=dev)
+    work_rows = 8 * torch.cuda.get_device_properties(dev).multi_processor_count
+    work = torch.empty((work_rows, n), dtype=torch.float64, device=dev)
+    L = _native.load()
+    s = torch.cuda.current_stream()
+
+    def launch():
+        _native.check(L.rkb_grid_pair_dot_batch(d["P"].data_ptr(), d["Q"].data_ptr(), d["P"].data_ptr(),
+                                                d["Q"].data_ptr(), n, d["a"].data_ptr(), d["b"].data_ptr(),
+                                                d["k"].data_ptr(), d["ok"].data_ptr(), rows, d["W"].data_ptr(), n,
+                                                d["ptr"].data_ptr(), d["cons"].data_ptr(), tab.r.data_ptr(), n,
+                                                tab.RK.data_ptr(), tab.inverse.data_ptr(), tab.cuts.data_ptr(),
+                                                tab.ncuts, tab.transfers.data_ptr(), tab.ntr, n - 1, val.data_ptr(),
+                                                work.data_ptr(), work_rows, _native.stream_handle(s)),
+                      "rkb_grid_pair_dot_batch")
+
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for e0, e1 in ev:
+        e0.record(s)
+        launch()
+        e1.record(s)
+    torch.cuda.synchronize()
+    ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
+    # host: the reference algorithm on a sample of rows, all threads
+    sample = min(rows, 256)
+    t0 = time.perf_counter()
+    ref = oracle.yk_pair_dot_batch_on_grid(P, Q, P, Q, a[:sample], b[:sample], ks[:sample], ok[:sample], W,
+                                           ptr[:sample + 1], cons[:2 * sample], r)
+    cpu_s = (time.perf_counter() - t0) * rows / sample
+    err = float(np.max(np.abs(val[:2 * sample].cpu().numpy() - ref)) / (np.abs(ref).max() + 1e-300))
+    # algorithmic bytes per row: P_a, P_b, Q_a, Q_b, rk, inverse, r read twice (two scans),
+    # y written and read back, the consumer rows read
+    bytes_row = 8 * n * (2 * 7 + 2 + 2)
+    return {"workload": f"{rows} pair rows, n={n} geometric grid, ranks 0..16, 2 consumers per row",
+            "rows_per_s": rows / (ms / 1e3), "ms_per_batch": ms, "cpu_rows_per_s": rows / cpu_s,
+            "cpu_cores": oracle.max_threads(), "cpu_sample_rows": sample,
+            "speedup_vs_cpu": cpu_s / (ms / 1e3), "max_rel_err_vs_oracle": err,
+            "algorithmic_gbs": bytes_row * rows / (ms / 1e3) / 1e9}
+
+
 def torch_sync():
     import torch
     torch.cuda.synchronize()
@@ -487,6 +559,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
     ap.add_argument("--serve", type=int, default=32, help="requests in the serving leg (0 = skip)")
+    ap.add_argument("--no-grid", action="store_true", help="skip the arbitrary-grid Y^k leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
