@@ -6,7 +6,7 @@
 * K3s tiles: equal (to FP64 rounding) to an exact int64 emulation of the
   residue GEMMs + CRT fed with the device's own residues.
 * End to end: Schwarz-relative error |R - R_ref| / sqrt(|R_acac R_bdbd|)
-  <= 1e-10 against the oracle (the BASELINE gate), with the measured maximum
+  <= 1e-10 against the oracle (the split engine's gate), with the measured maximum
   reported; the split table is symmetric and finite.
 """
 import os

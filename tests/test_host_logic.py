@@ -1,0 +1,82 @@
+"""CPU checks of the engines' host logic: task orders, split widths, row
+kernel choice, the cell-minor factor layout and the serving footprint."""
+import numpy as np
+import pytest
+
+
+def test_batch_tasks_cover_upper_tiles_and_lpt_orders_by_cost():
+    from atomx_b200.batch import batch_tasks
+    from atomx_b200.tables import tile_tasks
+    sizes, costs = [300, 1, 129, 0, 700], [896, 640, 1024, 512, 768]
+    ref = tile_tasks(sizes)
+    for order in ("group", "lpt"):
+        t = batch_tasks(sizes, costs, order)
+        assert sorted(map(tuple, t)) == sorted(map(tuple, ref))
+        assert np.all(t[:, 2] >= t[:, 1])
+    lpt = batch_tasks(sizes, costs, "lpt")
+    c = np.asarray(costs)[lpt[:, 0]]
+    assert np.all(np.diff(c) <= 0)
+    with pytest.raises(ValueError):
+        batch_tasks(sizes, costs, "random")
+
+
+def test_split_width_choice():
+    from atomx_b200.split import KDIM_MAX, check_kdim, choose_width
+    from atomx_b200.split_plan import MODULI, bits_for_moduli, moduli_needed
+    import math
+    for kdim in (128, 896, 1024, 2176, KDIM_MAX):
+        bits, n_mod = choose_width(None, None, kdim)
+        assert n_mod == moduli_needed(36, kdim) and bits >= 36
+        # the chosen width is exact: 2 kdim 2^(2 bits) + 2 < M
+        assert 2 * kdim * (1 << (2 * bits)) + 2 < math.prod(MODULI[:n_mod])
+        assert bits == max(36, bits_for_moduli(n_mod, kdim))
+    assert choose_width(30, None, 896) == (30, moduli_needed(30, 896))
+    with pytest.raises(ValueError):
+        check_kdim(KDIM_MAX + 128)
+
+
+def test_row_kernel_fit_rules():
+    from atomx_b200.split import cells_fit, fused_body_positions, fused_body_width, fused_fits
+    assert cells_fit(112, 8, 37) and cells_fit(192, 11, 64) and not cells_fit(200, 11, 64)
+    assert not cells_fit(100, 4, 0) and not cells_fit(100, 12, 0)
+    assert fused_fits(112, 8, 37) and not fused_fits(192, 11, 10)
+    for nv, ng in [(112, 8), (34, 7), (60, 5), (30, 11)]:
+        pos = fused_body_positions(nv, ng)
+        assert len(np.unique(pos)) == (nv - 1) * ng and pos.max() < fused_body_width(nv, ng)
+
+
+def test_cell_minor_tables_are_transposes_of_the_packed_ones():
+    from atomx_b200 import workloads as W
+    from atomx_b200.split import host_tables
+    from atomx_b200.split_plan import factor_table_layout
+    ion = W.build_ion(W.neon_small())
+    gr = ion.bsp["gr"]
+    nv, ng = gr.shape
+    H = host_tables(gr.ravel(), ng, [0, 1, 2])
+    o = factor_table_layout(nv, ng)
+    n = nv * ng
+    for k in (0, 1, 2):
+        F = H["flat"][H["koff"][k]:]
+        T = H["flat_t"][H["koff_t"][k]:]
+        u, ell = F[:n].reshape(nv, ng), F[o["ell"]:o["ell"] + n].reshape(nv, ng)
+        L = F[o["Lb"]:o["Lb"] + nv * ng * ng].reshape(nv, ng, ng)
+        C = F[o["C"]:o["C"] + n].reshape(nv, ng)
+        np.testing.assert_array_equal(T[:n].reshape(ng, nv), u.T)
+        np.testing.assert_array_equal(T[n:2 * n].reshape(ng, nv), ell.T)
+        np.testing.assert_array_equal(T[2 * n:3 * n].reshape(ng, nv), C.T)
+        np.testing.assert_array_equal(T[3 * n:3 * n + nv * ng * ng].reshape(ng, ng, nv), L.transpose(1, 2, 0))
+    assert host_tables(gr.ravel(), ng, [0, 1, 2]) is H  # cached
+
+
+def test_serving_footprint_grows_with_the_request():
+    from atomx_b200 import plan as PL
+    from atomx_b200 import workloads as W
+    from atomx_b200.serve import footprint_bytes
+    small = W.build_ion(W.neon_small())
+    big = W.build_ion(W.ytterbium_scaleup())
+    fs = footprint_bytes(small, PL.make_plan(small.kappa, 2), "split")
+    fb = footprint_bytes(big, PL.make_plan(big.kappa, 12), "split")
+    ff = footprint_bytes(big, PL.make_plan(big.kappa, 12), "fp64")
+    assert 0 < fs < fb and ff > 0
+    # the split estimate covers the residue matrices of that ion (11 moduli, two copies)
+    assert fb > 2 * 11 * 56209 * 1024
