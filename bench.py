@@ -185,7 +185,10 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": plan.ordered_entries / v * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Dirac-Coulomb spinors)",
-            "config": {"workload": WORKLOAD, "entries_per_step": plan.ordered_entries},
+            "config": {"workload": WORKLOAD, "engine": "reference algorithm (oracle C port), host cores",
+                       "k_max": spec.k_max, "entries_per_step": plan.ordered_entries,
+                       "unique_entries_per_step": plan.unique_entries, "rows": plan.n_rows,
+                       "parallelism": "rank 0 only (host)"},
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
