@@ -41,7 +41,7 @@ class ClockSampler:
     NAMES = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
              0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index: int, period: float = 0.05):
+    def __init__(self, index: int, period: float = 0.005):
         self.index, self.period = index, period
         self.samples, self.reasons = [], set()
         self.max_mhz = None
@@ -58,22 +58,26 @@ class ClockSampler:
         except Exception:
             self._nv = None
             return self
+        self._sample()  # one sample at the start of the timed region
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         return self
 
-    def _run(self):
+    def _sample(self):
         nv = self._nv
+        try:
+            self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+            for b, name in self.NAMES.items():
+                if bits & b:
+                    self.reasons.add(name)
+        except Exception:
+            pass
+
+    def _run(self):
         while not self._stop.is_set():
-            try:
-                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
-                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
-                for b, name in self.NAMES.items():
-                    if bits & b:
-                        self.reasons.add(name)
-            except Exception:
-                pass
             self._stop.wait(self.period)
+            self._sample()
 
     def __exit__(self, *exc):
         self._stop.set()
@@ -553,7 +557,7 @@ def torch_sync():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--engine", default=os.environ.get("RKB_ENGINE", "split"), choices=["split", "fp64"])
