@@ -32,9 +32,10 @@ import numpy as np
 import torch
 
 from . import _native
-from .split import IonRows, _round_up, check_kdim, choose_width
+from .split import (CB_STRIDE, CERT_LIMIT, IonRows, _round_up, certify, check_kdim, choose_width, join_stream,
+                    launch_stream)
 from .split_plan import crt_constants
-from .tables import TILE, IonDevice, RkTables, tile_tasks
+from .tables import TILE, IonDevice, RkTables, fp64_group_table, tile_tasks
 
 __all__ = ["SplitBatch", "Fp64Batch", "batch_tasks"]
 
@@ -73,8 +74,10 @@ class _Graphable:
         return g
 
     def replay(self):
+        """Replay the captured step on the current stream."""
         if self.graph is None:
             self.capture()
+        self._stream = torch.cuda.current_stream()
         self.graph.replay()
 
 
@@ -84,7 +87,8 @@ class SplitBatch(_Graphable):
     dominant_kernel = "split::crt_syrk_kernel"
 
     def __init__(self, devs: list[IonDevice], bits: int | None = None, tau: float = 1e-3, fused=None,
-                 corr_floor: float | None = None, order: str = "lpt", n_mod: int | None = None):
+                 corr_floor: float | None = None, order: str = "lpt", n_mod: int | None = None,
+                 cert_limit: float = CERT_LIMIT):
         _native.require_device()
         if not devs:
             raise ValueError("empty batch")
@@ -95,7 +99,7 @@ class SplitBatch(_Graphable):
         check_kdim(self.kpad)
         self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
-        self.cw = max(dv.ng for dv in self.devs)
+        self.cw = max(dv.ng for dv in self.devs) + 2  # g_0 and the two coupling moments
         self.cwp = _round_up(self.cw, 2)
         counts = [dv.plan.n_rows for dv in self.devs]
         self.row_base = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
@@ -106,7 +110,7 @@ class SplitBatch(_Graphable):
         self.rowscale = torch.empty(nrows, dtype=torch.float64, device=d)
         self.left = torch.zeros((nrows, self.cwp), dtype=torch.float64, device=d)
         self.right = torch.zeros_like(self.left)
-        self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
+        self.cbound = torch.empty((nrows, CB_STRIDE), dtype=torch.float64, device=d)
         two = [dv.plan.n_rows for dv, r in zip(self.devs, self.ions) if r.kind == "two"]
         self.xwork = torch.empty((max(two), self.kpad), dtype=torch.float64, device=d) if two else None
         self.corr_floor = 2.0 ** -(self.bits + 10) if corr_floor is None else float(corr_floor)
@@ -128,7 +132,13 @@ class SplitBatch(_Graphable):
         tasks = batch_tasks(g_n, g_kdim, order)
         self.n_tasks = int(tasks.shape[0])
         self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
-        self.status = torch.zeros(1, dtype=torch.int32, device=d)
+        #: [contraction status, number of tables whose certificate failed]
+        self.status = torch.zeros(2, dtype=torch.int32, device=d)
+        self.est = torch.zeros(len(g_n), dtype=torch.float64, device=d)
+        self.cert_limit = float(cert_limit)
+        #: (ion, k) tables recomputed in FP64 by the last check_status()
+        self.escalated: list = []
+        self._stream = None
         self.out = torch.empty(self.total, dtype=torch.float64, device=d)
         self._c = (np.ctypeslib.as_ctypes(np.ascontiguousarray(self.moduli, dtype=np.int32)),
                    np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_hi)),
@@ -137,17 +147,21 @@ class SplitBatch(_Graphable):
 
     @property
     def launches_per_step(self) -> int:
-        return sum(2 if r.kind == "two" else 1 for r in self.ions) + 1
+        """Row kernels of every ion, the certificate and the contraction."""
+        return sum(2 if r.kind == "two" else 1 for r in self.ions) + 2
 
     @property
     def ordered_entries(self) -> int:
         return sum(dv.plan.ordered_entries for dv in self.devs)
 
     def rows(self, stream=None) -> None:
+        self._stream = stream
         for i, r in enumerate(self.ions):
             r.launch(self.bits, self.n_mod, self._c[0], self.resA, self.resB, self.kpad, int(self.row_base[i]),
                      self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp, self.xwork,
                      stream)
+        certify(self.grp_row0, self.grp_n, self.rowscale, self.cbound, self.cert_limit, self.est, self.status,
+                stream)
 
     def contract(self, stream=None) -> None:
         L = _native.load()
@@ -167,10 +181,21 @@ class SplitBatch(_Graphable):
         self.contract(stream)
 
     def check_status(self) -> None:
-        st = int(self.status.item())
+        """Wait for the device, raise a contraction error, and recompute in FP64
+        every (ion, k) table whose certificate failed (listed in ``escalated``)."""
+        s = launch_stream(self._stream)
+        st, flagged = self.status.tolist()
         if st:
-            self.status.zero_()
+            self.status[0] = 0
             _native.check(st, "crt_syrk_kernel")
+        self.escalated = []
+        if flagged:
+            est = self.est.cpu().numpy()
+            for j, (i, k) in enumerate(self.group_of):
+                if not est[j] <= self.cert_limit:
+                    fp64_group_table(self.devs[i], k, self.table(i, k).reshape(-1), s)
+                    self.escalated.append((i, k))
+            join_stream(s)
 
     def table(self, ion: int, k: int) -> torch.Tensor:
         nk = self.devs[ion].plan.n_of_k(k)
@@ -188,6 +213,7 @@ class SplitBatch(_Graphable):
     def info(self) -> dict:
         return {"ions": len(self.devs), "bits": self.bits, "n_mod": self.n_mod, "kpad": self.kpad,
                 "order": self.order, "tasks": self.n_tasks, "rows": int(self.row_base[-1]),
+                "cert_limit": self.cert_limit, "fp64_tables": [list(t) for t in self.escalated],
                 "row_kernels": {kd: sum(r.kind == kd for r in self.ions) for kd in ("cells", "fused", "two")},
                 "entries": self.ordered_entries}
 

@@ -10,12 +10,15 @@
 //     c_m = L_m^-1 (v_m - sigma u_m),  sigma += |c_m|^2,
 // where Delta_m = sum_e z_e z_e^T lifts every eigenvalue of the diagonally
 // scaled S_m below tau * lambda_max to max(|lambda|, tau lambda_max); the z_e
-// become the negative-sign columns Z.  Then ell_m = L_m^-1 u_m (1 - sum
-// c.ell) carries the core-body coupling, and S_c = G_00 - |ell|^2 v_0 v_0^T
-// is the FP64 core term.  This is the same factorisation as
-// atomx_b200.split_plan.green_factor (numpy); the eigenproblems here are
-// solved by cyclic Jacobi rotations (ng <= 32), so eigenvector signs may
-// differ, which leaves every z_e z_e^T and the factor unchanged.
+// become the negative-sign columns Z.  The core cell 0 stays in FP64: its
+// block G_00 and the rank-one core-body coupling v_0 u_b^T, which the row
+// kernels carry as the two scaled moments alpha*sx = sx v_0.g_0 and
+// q/sx = u_b.g_b / sx.  sx = r_b^-(k+1)/2 r_l^-k/2 (r_l the last core node,
+// r_b the first body node) bounds both by |g|_1 / sqrt(r_b).  This is the
+// same factorisation as atomx_b200.split_plan.green_factor (numpy); the
+// eigenproblems here are solved by cyclic Jacobi rotations (ng <= 32), so
+// eigenvector signs may differ, which leaves every z_e z_e^T and the factor
+// unchanged.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -105,9 +108,9 @@ extern "C" long rkb_green_factor(const double *r, int nv, int ng, int k, double 
     RKB_CHECK_ARG(nv >= 2 && ng >= 1 && ng <= RKB_MAX_NG, "invalid grid (nv=%d, ng=%d)", nv, ng);
     RKB_CHECK_ARG(k >= 0 && tau >= 0.0, "invalid multipole or shift threshold");
     const int n = nv * ng, g2 = ng * ng;
-    const long fixed = 2L * n + (long)nv * g2 + (long)nv * ng + ng + g2 + 1;
+    const long fixed = (long)n + (long)nv * g2 + (long)nv * ng + ng + g2 + 2;
     RKB_CHECK_ARG(cap >= fixed, "output capacity %ld below the %ld fixed doubles", cap, fixed);
-    std::vector<double> u(n), v(n), ell(n, 0.0), Lb((size_t)nv * g2, 0.0), C((size_t)nv * ng, 0.0);
+    std::vector<double> u(n), v(n), Lb((size_t)nv * g2, 0.0), C((size_t)nv * ng, 0.0);
     for (int i = 0; i < n; ++i) {
         u[i] = std::pow(r[i], -(double)(k + 1));
         v[i] = std::pow(r[i], (double)k);
@@ -169,33 +172,20 @@ extern "C" long rkb_green_factor(const double *r, int nv, int ng, int k, double 
         plan::lower_solve(ng, Lm, rhs.data(), Cm);
         for (int i = 0; i < ng; ++i) sigma += Cm[i] * Cm[i];
     }
-    double s_acc = 0.0, ell2 = 0.0;
-    for (int m = 1; m < nv; ++m) {
-        for (int i = 0; i < ng; ++i) rhs[i] = u[(size_t)m * ng + i] * (1.0 - s_acc);
-        double *em = &ell[(size_t)m * ng];
-        plan::lower_solve(ng, &Lb[(size_t)m * g2], rhs.data(), em);
-        for (int i = 0; i < ng; ++i) {
-            s_acc += C[(size_t)m * ng + i] * em[i];
-            ell2 += em[i] * em[i];
-        }
-    }
     const long nz = (long)zcell.size();
     const long total = fixed + nz * (ng + 1);
     RKB_CHECK_ARG(cap >= total, "output capacity %ld below the %ld doubles of this factor", cap, total);
-    // u[N] | ell[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] | Sc[ng][ng] | nZ | nZ x (cell, z[ng])
+    // u[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] | G00[ng][ng] | sx | nZ | nZ x (cell, z[ng])
     double *o = out;
     std::memcpy(o, u.data(), sizeof(double) * n); o += n;
-    std::memcpy(o, ell.data(), sizeof(double) * n); o += n;
     std::memcpy(o, Lb.data(), sizeof(double) * (size_t)nv * g2); o += (size_t)nv * g2;
     std::memcpy(o, C.data(), sizeof(double) * (size_t)nv * ng); o += (size_t)nv * ng;
     for (int i = 0; i < ng; ++i) o[i] = v[i];
     o += ng;
     for (int i = 0; i < ng; ++i)
-        for (int j = 0; j < ng; ++j) {
-            const double gcc = u[i] * v[j] * mo[i * ng + j] + v[i] * u[j] * mi[i * ng + j];
-            o[i * ng + j] = gcc - ell2 * v[i] * v[j];
-        }
+        for (int j = 0; j < ng; ++j) o[i * ng + j] = u[i] * v[j] * mo[i * ng + j] + v[i] * u[j] * mi[i * ng + j];
     o += g2;
+    *o++ = std::sqrt(u[ng]) / std::sqrt(v[ng - 1]);  // sx (k = 0: v = 1)
     *o++ = (double)nz;
     for (long e = 0; e < nz; ++e) {
         *o++ = (double)zcell[e];

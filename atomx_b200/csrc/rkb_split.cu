@@ -6,12 +6,17 @@
 // K2x  split_rows_kernel  (one warp per (pair, k) row, FP64 on CUDA cores)
 //      g = w (P_a P_c + Q_a Q_c);  per body cell m >= 1:  d_m = u_m . g_m and
 //      the exclusive suffix sums T_m = sum_{m'>m} d_m' (warp-shuffle scans);
-//      X_m = L_mm^T g_m + c_m T_m + ell_m (v_0.g_0);  Z_e = z_e . g_{cell(e)};
-//      FP64 core terms left = g_0, right = S_c g_0 (core Schur complement).
+//      X_m = L_mm^T g_m + c_m T_m;  Z_e = z_e . g_{cell(e)};
+//      FP64 core terms left = [g_0, alpha sx, q/sx], right = [G_00 g_0, q/sx,
+//      alpha sx] with alpha = v_0.g_0 and q = T_0 (the core-body coupling).
 //      The FP64 row [X | Z] goes to a scratch buffer with its power-of-two
 //      scale (|x| < 2^bits); split_residues_kernel then rounds it to integers
 //      x~ and writes int8 residues x~ mod m_i (and the B copy with Z negated)
 //      in a [modulus][row][kpad] layout, one 16-byte store per modulus.
+//      Per row the kernels also record (cbound, CB_STRIDE doubles): the
+//      screen bounds |g_0|, |G_00 g_0|, |alpha sx|, |q/sx| relative to the row
+//      scale, and for the certificate |[X | Z]| and the FP64 diagonal
+//      R_aa = |X|^2 - |Z|^2 + left.right.
 //
 // K3s  crt_syrk_kernel  (persistent, one CTA per SM, 18 warps)
 //      warp 0: TMA producer — 128x128-byte boxes (SWIZZLE_128B) of the A and B
@@ -31,6 +36,8 @@
 //      RKB_ETIMEDOUT in *status and every role drains and returns.
 #include <cuda.h>
 
+#include <cfloat>
+
 #include <mutex>
 
 #include "rkb_common.cuh"
@@ -39,6 +46,24 @@ namespace rkb {
 namespace split {
 
 constexpr int MAXMOD = 12;
+// Doubles per row of the cbound array: [0] |g_0|, [1] |G_00 g_0|, [2] |alpha sx|,
+// [3] |q/sx| (each times 2^-e of the row scale), [4] |[X | Z]|, [5] R_aa, [6..7] 0.
+constexpr int CB_STRIDE = 8;
+
+// The per-row record: screen bounds relative to 2^-e (infinite for a zero
+// row, which is never screened), the row norm and the FP64 diagonal.
+__device__ __forceinline__ void write_row_record(double *cb, double amax, int ex, double n_g0, double n_gg,
+                                                 double a_sx, double q_sx, double xsq, double zsq, double g0gg) {
+    const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
+    cb[0] = sqrt(n_g0) * rel;
+    cb[1] = sqrt(n_gg) * rel;
+    cb[2] = fabs(a_sx) * rel;
+    cb[3] = fabs(q_sx) * rel;
+    cb[4] = sqrt(xsq + zsq);
+    cb[5] = xsq - zsq + g0gg + 2.0 * a_sx * q_sx;
+    cb[6] = 0.0;
+    cb[7] = 0.0;
+}
 
 // =========================================================================
 // K2x — transform, quantise, residues
@@ -113,13 +138,13 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
     const int k = a.row_k[q];
     const double *tab = a.ktab + a.koff[k];
     const double *u = tab;
-    const double *ell = u + n;
-    const double *Lb = ell + n;
+    const double *Lb = u + n;
     const double *C = Lb + (long)nv * ng * ng;
     const double *v0 = C + (long)nv * ng;
-    const double *Sc = v0 + ng;
-    const int nz = (int)Sc[ng * ng];
-    const double *zt = Sc + ng * ng + 1;
+    const double *G00 = v0 + ng;
+    const double sx = G00[ng * ng];
+    const int nz = (int)G00[ng * ng + 1];
+    const double *zt = G00 + ng * ng + 2;
     const long kbody = (long)(nv - 1) * ng;
     // lane groups: cpp cells per pass, lane -> (cell offset, node)
     const int cpp = 32 / ng;
@@ -128,7 +153,7 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
 
     for (long i = lane; i < n; i += 32) g[i] = __dmul_rn(a.w[i], rho_at(a, q, i));
     __syncwarp();
-    // alpha = v_0 . g_0: the core charge moment that couples into every X
+    // alpha = v_0 . g_0: the core multipole moment of the core-body coupling
     double alpha = 0.0;
     for (int j = lane; j < ng; j += 32) alpha = fma(v0[j], g[j], alpha);
     alpha = warp_sum(alpha);
@@ -158,20 +183,21 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
     }
     __syncwarp();
 
-    // the row [X | Z | 0...] into the scratch row, with its maximum
+    // the row [X | Z | 0...] into the scratch row, with its maximum and sums of squares
     const long grow = a.row_base + q;  // row index in the residue matrices
     double *xs = a.xwork + grow * a.kpad;
-    double amax = 0.0;
+    double amax = 0.0, xsq = 0.0, zsq = 0.0;
     bool bad = false;  // fmax drops NaNs, so non-finite values are tracked apart
     for (int m0 = 1; m0 < nv; m0 += cpp) {
         const int m = m0 + sub;
         if (glane && m < nv) {
             const double *L = Lb + (long)m * ng * ng;
             const double *gm = g + (long)m * ng;
-            double x = fma(ell[(long)m * ng + node], alpha, C[(long)m * ng + node] * tsuf[m]);
+            double x = C[(long)m * ng + node] * tsuf[m];
             for (int i = node; i < ng; ++i) x = fma(L[i * ng + node], gm[i], x);
             xs[(long)(m - 1) * ng + node] = x;
             amax = fmax(amax, fabs(x));
+            xsq = fma(x, x, xsq);
             bad |= !isfinite(x);
         }
     }
@@ -182,10 +208,13 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
         for (int i = 0; i < ng; ++i) x = fma(ze[1 + i], gm[i], x);
         xs[kbody + e] = x;
         amax = fmax(amax, fabs(x));
+        zsq = fma(x, x, zsq);
         bad |= !isfinite(x);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    xsq = warp_sum(xsq);
+    zsq = warp_sum(zsq);
 
     for (long c = kbody + nz + lane; c < a.kpad; c += 32) xs[c] = 0.0;
     int ex = 0;
@@ -195,32 +224,38 @@ __global__ void __launch_bounds__(128) split_rows_kernel(RowsArgs a) {
         inv_scale = ldexp(1.0, ex - a.bits);
     }
 
-    // FP64 core correction: left = g_0, right = S_c g_0, and the screen bounds
+    // FP64 core terms: left = [g_0, alpha sx, q/sx], right = [G_00 g_0, q/sx, alpha sx]
+    const double a_sx = alpha * sx, q_sx = tsuf[0] / sx;  // T_0 = u_b . g_b
+    bad |= !isfinite(a_sx) || !isfinite(q_sx);
     double *lf = a.left + grow * a.cwp, *rt = a.right + grow * a.cwp;
-    double n1 = 0.0, n2 = 0.0;
+    double n1 = 0.0, n2 = 0.0, gg = 0.0;
     for (int i = lane; i < a.cwp; i += 32) {
         double gi = 0.0, sacc = 0.0;
         if (i < ng) {
             gi = g[i];
-            for (int j = 0; j < ng; ++j) sacc = fma(Sc[i * ng + j], g[j], sacc);
+            for (int j = 0; j < ng; ++j) sacc = fma(G00[i * ng + j], g[j], sacc);
+            n1 = fma(gi, gi, n1);
+            n2 = fma(sacc, sacc, n2);
+            gg = fma(gi, sacc, gg);
+        } else if (i == ng) {
+            gi = a_sx;
+            sacc = q_sx;
+        } else if (i == ng + 1) {
+            gi = q_sx;
+            sacc = a_sx;
         }
         lf[i] = gi;
         rt[i] = sacc;
-        n1 = fma(gi, gi, n1);
-        n2 = fma(sacc, sacc, n2);
     }
     n1 = warp_sum(n1);
     n2 = warp_sum(n2);
+    gg = warp_sum(gg);
     bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
         // a non-finite row gets a NaN scale: its residues are zero and every
         // entry it reaches is NaN, which the contraction reports
         a.rowscale[grow] = bad ? __longlong_as_double(0x7ff8000000000000LL) : inv_scale;
-        // bounds of |g_0| and |S_c g_0| relative to 2^ex (>= the row maximum of
-        // |[X | Z]|); a zero row keeps them infinite (never screened)
-        const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
-        a.cbound[grow * 2] = sqrt(n1) * rel;
-        a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+        write_row_record(a.cbound + grow * CB_STRIDE, amax, ex, n1, n2, a_sx, q_sx, xsq, zsq, gg);
     }
 }
 
@@ -332,13 +367,13 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
     const long n = (long)nv * NG;
     const double *tab = a.ktab + a.koff[k];
     const double *u = tab;
-    const double *ell = u + n;
-    const double *Lb = ell + n;
+    const double *Lb = u + n;
     const double *C = Lb + (long)nv * NG * NG;
     const double *v0 = C + (long)nv * NG;
-    const double *Sc = v0 + NG;
-    const int nz = (int)Sc[NG * NG];
-    const double *zt = Sc + NG * NG + 1;
+    const double *G00 = v0 + NG;
+    const double sx = G00[NG * NG];
+    const int nz = (int)G00[NG * NG + 1];
+    const double *zt = G00 + NG * NG + 2;
     const int sub = lane / NG, node = lane - sub * NG;
     const bool glane = sub < CPP;
     const long grow = a.row_base + q;
@@ -346,25 +381,21 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
         return __dmul_rn(a.w[i], __dadd_rn(__dmul_rn(Pa[i], Pc[i]), __dmul_rn(Qa[i], Qc[i])));
     };
 
-    // cell 0: g_0 (lanes < NG), alpha = v_0 . g_0, core vectors and their norms
+    // cell 0: g_0 (lanes < NG), alpha = v_0 . g_0, G_00 g_0 and their norms
     const double g0 = lane < NG ? gval(lane) : 0.0;
     const double alpha = warp_sum(lane < NG ? v0[lane] * g0 : 0.0);
     double sg = 0.0;
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
         const double gj = __shfl_sync(FULL, g0, j);
-        if (lane < NG) sg = fma(Sc[lane * NG + j], gj, sg);
+        if (lane < NG) sg = fma(G00[lane * NG + j], gj, sg);
     }
-    if (lane < a.cwp) {
-        a.left[grow * a.cwp + lane] = g0;
-        a.right[grow * a.cwp + lane] = sg;
-    }
-    const double n1 = warp_sum(g0 * g0), n2 = warp_sum(sg * sg);
+    const double n1 = warp_sum(g0 * g0), n2 = warp_sum(sg * sg), gg = warp_sum(g0 * sg);
 
     // body passes, last cell first
     const int P = (int)fused_passes(nv, NG);
     double xs[FUSED_PMAX];
-    double carry = 0.0, amax = 0.0;
+    double carry = 0.0, amax = 0.0, xsq = 0.0, zsq = 0.0;
     bool bad = false;
 #pragma unroll
     for (int p = 0; p < FUSED_PMAX; ++p) {
@@ -393,7 +424,7 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
             const double t = carry + before;
             carry += all;
             const double *L = Lb + (long)m * NG * NG;
-            double x = ok ? fma(ell[i], alpha, C[i] * t) : 0.0;
+            double x = ok ? C[i] * t : 0.0;
 #pragma unroll
             for (int ii = 0; ii < NG; ++ii) {
                 const double gi = __shfl_sync(FULL, g, (sub * NG + ii) & 31);
@@ -401,8 +432,17 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
             }
             xs[p] = x;
             amax = fmax(amax, fabs(x));
+            xsq = fma(x, x, xsq);
             bad |= !isfinite(x);
         }
+    }
+    // core terms: left = [g_0, alpha sx, q/sx], right = [G_00 g_0, q/sx, alpha sx]
+    // (the carry now holds q = u_b . g_b on every lane)
+    const double a_sx = alpha * sx, q_sx = carry / sx;
+    bad |= !isfinite(a_sx) || !isfinite(q_sx);
+    if (lane < a.cwp) {
+        a.left[grow * a.cwp + lane] = lane < NG ? g0 : (lane == NG ? a_sx : (lane == NG + 1 ? q_sx : 0.0));
+        a.right[grow * a.cwp + lane] = lane < NG ? sg : (lane == NG ? q_sx : (lane == NG + 1 ? a_sx : 0.0));
     }
     // Z columns: lane e and e + 32
     double zx[2] = {0.0, 0.0};
@@ -416,11 +456,14 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
             for (int ii = 0; ii < NG; ++ii) x = fma(ze[1 + ii], gval(base + ii), x);
             zx[h] = x;
             amax = fmax(amax, fabs(x));
+            zsq = fma(x, x, zsq);
             bad |= !isfinite(x);
         }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(FULL, amax, o));
+    xsq = warp_sum(xsq);
+    zsq = warp_sum(zsq);
     bad = __any_sync(FULL, bad);
     int ex = 0;
     double scale = 0.0, inv_scale = 0.0;
@@ -431,9 +474,7 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
     }
     if (lane == 0) {
         a.rowscale[grow] = bad ? __longlong_as_double(0x7ff8000000000000LL) : inv_scale;
-        const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
-        a.cbound[grow * 2] = sqrt(n1) * rel;
-        a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+        write_row_record(a.cbound + grow * CB_STRIDE, amax, ex, n1, n2, a_sx, q_sx, xsq, zsq, gg);
     }
 
     // quantise in place (exact integers, |x| <= 2^bits) and write residues
@@ -482,14 +523,14 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
 // (consecutive threads, consecutive nodes) into a padded shared-memory image;
 // each thread then reads its cell's g and the cell-minor factor copy
 // (entry i of every cell contiguous, so a warp's reads are consecutive) and
-// forms X = L_m^T g_m + C_m t_m + ell_m alpha in registers, without shuffles.
+// forms X = L_m^T g_m + C_m t_m in registers, without shuffles.
 // Threads past the cells compute the Z columns.  After a block maximum fixes
 // the row's power-of-two scale, every thread writes its int8 residues into
 // per-modulus row images in shared memory, and the block copies them out with
 // 16-byte stores.  Columns are in natural order: (m-1)*ng + node, then Z.
 //
 // Cell-minor factor table of one multipole (doubles), nv cells:
-//   u[NG][nv] | ell[NG][nv] | C[NG][nv] | L[NG][NG][nv] (L[i][node][m])
+//   u[NG][nv] | C[NG][nv] | L[NG][NG][nv] (L[i][node][m])
 template <int NG>
 __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const double *__restrict__ ktab_t,
                                                               const long *__restrict__ koff_t) {
@@ -499,10 +540,9 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
     const long q = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
     const long kpad = a.kpad;
-    const size_t ndbl = ((size_t)nv * GS + 66 + 1) & ~(size_t)1;     // doubles before the images (even: 16-B aligned)
+    const size_t ndbl = ((size_t)nv * GS + 64 + 1) & ~(size_t)1;     // doubles before the images (even: 16-B aligned)
     double *gimg = reinterpret_cast<double *>(smc);                  // [nv][GS]
     double *red = gimg + (size_t)nv * GS;                              // [64] block scratch
-    double *bcast = red + 64;                                          // alpha
     unsigned char *lines = smc + ndbl * sizeof(double);               // [n_mod][kpad]
     unsigned char *zneg = lines + (size_t)a.n_mod * kpad;             // [n_mod][64]: B's Z bytes
     const int k = a.row_k[q];
@@ -511,12 +551,13 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
     const double *Qa = a.Q + a.pairs[2 * pr] * a.orb_ld, *Qc = a.Q + a.pairs[2 * pr + 1] * a.orb_ld;
     const long n = (long)nv * NG;
     const double *tab = a.ktab + a.koff[k];
-    const double *v0 = tab + 2 * n + (long)nv * NG * NG + (long)nv * NG;
-    const double *Sc = v0 + NG;
-    const int nz = (int)Sc[NG * NG];
-    const double *zt = Sc + NG * NG + 1;
+    const double *v0 = tab + n + (long)nv * NG * NG + (long)nv * NG;
+    const double *G00 = v0 + NG;
+    const double sx = G00[NG * NG];
+    const int nz = (int)G00[NG * NG + 1];
+    const double *zt = G00 + NG * NG + 2;
     const double *tt = ktab_t + koff_t[k];
-    const double *ut = tt, *ellt = tt + n, *Ct = tt + 2 * n, *Lt = tt + 3 * n;
+    const double *ut = tt, *Ct = tt + n, *Lt = tt + 2 * n;
     const long kbody = (long)(nv - 1) * NG;
     const long grow = a.row_base + q;
     // g = w * (P_a P_c + Q_a Q_c) for the whole row, coalesced
@@ -537,24 +578,23 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
             for (int i = 0; i < NG; ++i) d = fma(ut[(long)i * nv + m], g[i], d);
         }
     }
-    // cell 0: alpha = v_0 . g_0, core vectors and their norms (one thread)
-    double n1 = 0.0, n2 = 0.0;
+    // cell 0: alpha = v_0 . g_0, G_00 g_0 and their norms (one thread)
+    double n1 = 0.0, n2 = 0.0, gg = 0.0, alpha = 0.0;
     if (m == 0) {
-        double al = 0.0;
 #pragma unroll
-        for (int i = 0; i < NG; ++i) al = fma(v0[i], g[i], al);
-        *bcast = al;
+        for (int i = 0; i < NG; ++i) alpha = fma(v0[i], g[i], alpha);
 #pragma unroll
         for (int i = 0; i < NG; ++i) {
             double sacc = 0.0;
 #pragma unroll
-            for (int j = 0; j < NG; ++j) sacc = fma(Sc[i * NG + j], g[j], sacc);
+            for (int j = 0; j < NG; ++j) sacc = fma(G00[i * NG + j], g[j], sacc);
             a.left[grow * a.cwp + i] = g[i];
             a.right[grow * a.cwp + i] = sacc;
             n1 = fma(g[i], g[i], n1);
             n2 = fma(sacc, sacc, n2);
+            gg = fma(g[i], sacc, gg);
         }
-        for (int i = NG; i < a.cwp; ++i) a.left[grow * a.cwp + i] = a.right[grow * a.cwp + i] = 0.0;
+        for (int i = NG + 2; i < a.cwp; ++i) a.left[grow * a.cwp + i] = a.right[grow * a.cwp + i] = 0.0;
     }
     // exclusive scan of d over threads (= suffix sums over cells)
     const double incl = warp_inclusive_scan(d, lane);
@@ -564,19 +604,30 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
     for (int w = 0; w < wid; ++w) before += red[w];
     const double up = __shfl_up_sync(0xffffffffu, incl, 1);
     const double t_m = lane == 0 ? before : before + up;
-    const double alpha = *bcast;
-    double amax = 0.0;
+    double amax = 0.0, xsq = 0.0, zsq = 0.0;
     bool bad = false;
     if (m >= 1) {
 #pragma unroll
         for (int node = 0; node < NG; ++node) {
-            double xv = fma(ellt[(long)node * nv + m], alpha, Ct[(long)node * nv + m] * t_m);
+            double xv = Ct[(long)node * nv + m] * t_m;
 #pragma unroll
             for (int i = node; i < NG; ++i) xv = fma(Lt[((long)i * NG + node) * nv + m], g[i], xv);
             x[node] = xv;
             amax = fmax(amax, fabs(xv));
+            xsq = fma(xv, xv, xsq);
             bad |= !isfinite(xv);
         }
+    }
+    // cell 0: the core-body coupling columns (t_0 = q = u_b . g_b)
+    double a_sx = 0.0, q_sx = 0.0;
+    if (m == 0) {
+        a_sx = alpha * sx;
+        q_sx = t_m / sx;
+        bad |= !isfinite(a_sx) || !isfinite(q_sx);
+        a.left[grow * a.cwp + NG] = a_sx;
+        a.left[grow * a.cwp + NG + 1] = q_sx;
+        a.right[grow * a.cwp + NG] = q_sx;
+        a.right[grow * a.cwp + NG + 1] = a_sx;
     }
     // Z columns: thread nv + e
     const int e = tid - nv;
@@ -587,22 +638,31 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
 #pragma unroll
         for (int i = 0; i < NG; ++i) zx = fma(ze[1 + i], gimg[cz * GS + i], zx);
         amax = fmax(amax, fabs(zx));
+        zsq = zx * zx;
         bad |= !isfinite(zx);
     }
-    // block maximum and non-finite flag
+    // block maximum, sums of squares and non-finite flag (red[]: 8 warps at most)
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    xsq = warp_sum(xsq);
+    zsq = warp_sum(zsq);
     const int badw = __any_sync(0xffffffffu, bad);
     __syncthreads();  // red[] reused
     if (lane == 0) {
         red[wid] = amax;
+        red[8 + wid] = xsq;
+        red[16 + wid] = zsq;
         red[32 + wid] = badw ? 1.0 : 0.0;
     }
     __syncthreads();
     amax = 0.0;
+    xsq = 0.0;
+    zsq = 0.0;
     bool anybad = false;
     for (int w = 0; w < nwarp; ++w) {
         amax = fmax(amax, red[w]);
+        xsq += red[8 + w];
+        zsq += red[16 + w];
         anybad |= red[32 + w] != 0.0;
     }
     int ex = 0;
@@ -614,9 +674,7 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
     }
     if (m == 0) {
         a.rowscale[grow] = anybad ? __longlong_as_double(0x7ff8000000000000LL) : inv_scale;
-        const double rel = amax > 0.0 ? ldexp(1.0, -ex) : INFINITY;
-        a.cbound[grow * 2] = sqrt(n1) * rel;
-        a.cbound[grow * 2 + 1] = sqrt(n2) * rel;
+        write_row_record(a.cbound + grow * CB_STRIDE, amax, ex, n1, n2, a_sx, q_sx, xsq, zsq, gg);
     }
     // residues into the row images (natural column order), zero tails
     const double rc = 6755399441055744.0;  // 1.5 * 2^52
@@ -965,21 +1023,35 @@ __global__ void __launch_bounds__(THREADS, 1)
             double *R = p.out + p.grp_out[g];
             // Correction screen for this warp's 32 x EPI_COLS block: with per-row bounds
             // relative to each row's scale, |left_a . right_b| <= 2^(e_a+e_b) *
-            // |g0_a| |S_c g0_b|.  Below corr_floor the term is far under the
-            // split's own error and is skipped.
-            double r1 = 0.0, c2 = 0.0;
-            if (arow) r1 = __ldg(p.cbound + (row0 + a) * 2);
+            // (|g0_a| |G00 g0_b| + |alpha_a sx| |q_b/sx| + |q_a/sx| |alpha_b sx|).
+            // Below corr_floor the term is far under the split's own error and is skipped.
+            double ra0 = 0.0, ra2 = 0.0, ra3 = 0.0, cb1 = 0.0, cb2 = 0.0, cb3 = 0.0;
+            if (arow) {
+                const double *cr = p.cbound + (row0 + a) * CB_STRIDE;
+                ra0 = __ldg(cr);
+                ra2 = __ldg(cr + 2);
+                ra3 = __ldg(cr + 3);
+            }
 #pragma unroll
             for (int h = 0; h < EPI_COLS / 32; ++h) {
                 const long bcol = b0 + lane + 32 * h;
-                if (bcol < n) c2 = fmax(c2, __ldg(p.cbound + (row0 + bcol) * 2 + 1));
+                if (bcol < n) {
+                    const double *cc = p.cbound + (row0 + bcol) * CB_STRIDE;
+                    cb1 = fmax(cb1, __ldg(cc + 1));
+                    cb2 = fmax(cb2, __ldg(cc + 2));
+                    cb3 = fmax(cb3, __ldg(cc + 3));
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
-                r1 = fmax(r1, __shfl_xor_sync(0xffffffffu, r1, o));
-                c2 = fmax(c2, __shfl_xor_sync(0xffffffffu, c2, o));
+                ra0 = fmax(ra0, __shfl_xor_sync(0xffffffffu, ra0, o));
+                ra2 = fmax(ra2, __shfl_xor_sync(0xffffffffu, ra2, o));
+                ra3 = fmax(ra3, __shfl_xor_sync(0xffffffffu, ra3, o));
+                cb1 = fmax(cb1, __shfl_xor_sync(0xffffffffu, cb1, o));
+                cb2 = fmax(cb2, __shfl_xor_sync(0xffffffffu, cb2, o));
+                cb3 = fmax(cb3, __shfl_xor_sync(0xffffffffu, cb3, o));
             }
-            const bool need_corr = !(r1 * c2 <= p.corr_floor);
+            const bool need_corr = !(ra0 * cb1 + ra2 * cb3 + ra3 * cb2 <= p.corr_floor);
             constexpr int FC = 8;  // columns per final-phase chunk
             // The final phase runs once per tile: a rolled loop keeps its code
             // small enough to stay in the instruction cache beside the
@@ -1116,7 +1188,7 @@ extern "C" int rkb_split_rows(const double *d_Pv, const double *d_Qv, long orb_l
     RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
     RKB_CHECK_ARG(kpad % BKB == 0 && kpad >= (long)(nv - 1) * ng, "kpad must be a multiple of %d >= body width",
                   BKB);
-    RKB_CHECK_ARG(cwp >= ng, "correction width must be >= ng");
+    RKB_CHECK_ARG(cwp >= ng + 2, "correction width must be >= ng + 2");
     RKB_CHECK_ARG(d_cbound != nullptr, "the correction-bound array is required");
     RKB_CHECK_ARG(row_base >= 0 && row_base + nrows <= nrows_total, "row range outside the residue matrices");
     if (nrows == 0) return RKB_OK;
@@ -1185,7 +1257,7 @@ extern "C" int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long
     RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
     RKB_CHECK_ARG(kpad % BKB == 0 && kpad >= (long)(nv - 1) * ng + max_z, "kpad must be a multiple of %d >= %ld",
                   BKB, (long)(nv - 1) * ng + max_z);
-    RKB_CHECK_ARG(cwp >= ng, "correction width must be >= ng");
+    RKB_CHECK_ARG(cwp >= ng + 2, "correction width must be >= ng + 2");
     RKB_CHECK_ARG(d_cbound != nullptr, "the correction-bound array is required");
     RKB_CHECK_ARG(row_base >= 0 && row_base + nrows <= nrows_total, "row range outside the residue matrices");
     RKB_CHECK_ARG(((uintptr_t)d_resA % 16) == 0 && (d_resB == nullptr || ((uintptr_t)d_resB % 16) == 0),
@@ -1204,7 +1276,7 @@ extern "C" int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long
     a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
     a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
     RKB_CHECK_ARG(d_ktab_t != nullptr && d_koff_t != nullptr, "the cell-minor factor tables are required");
-    const size_t smem = ((((size_t)nv * (ng | 1) + 66 + 1) & ~(size_t)1) * sizeof(double)) + (size_t)n_mod * (kpad + 64);
+    const size_t smem = ((((size_t)nv * (ng | 1) + 64 + 1) & ~(size_t)1) * sizeof(double)) + (size_t)n_mod * (kpad + 64);
     RKB_CHECK_ARG(smem <= 200 * 1024, "row images too large for shared memory");
     cudaStream_t st = as_stream(stream);
     const dim3 grid((unsigned)nrows), block((unsigned)threads);
@@ -1243,7 +1315,7 @@ extern "C" int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long
     RKB_CHECK_ARG(n_mod >= 1 && n_mod <= MAXMOD, "1..%d moduli supported (got %d)", MAXMOD, n_mod);
     RKB_CHECK_ARG(kpad % BKB == 0 && kpad >= fused_body_width(nv, ng) + max_z,
                   "kpad must be a multiple of %d >= %ld", BKB, fused_body_width(nv, ng) + max_z);
-    RKB_CHECK_ARG(cwp >= ng && cwp <= 32, "correction width must be in [ng, 32]");
+    RKB_CHECK_ARG(cwp >= ng + 2 && cwp <= 32, "correction width must be in [ng + 2, 32]");
     RKB_CHECK_ARG(d_cbound != nullptr, "the correction-bound array is required");
     RKB_CHECK_ARG(row_base >= 0 && row_base + nrows <= nrows_total, "row range outside the residue matrices");
     RKB_CHECK_ARG(((uintptr_t)d_resA % 16) == 0 && (d_resB == nullptr || ((uintptr_t)d_resB % 16) == 0),
@@ -1332,6 +1404,85 @@ extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *
     }
 #undef RKB_CRT_CASE
     RKB_LAUNCHED("crt_syrk_kernel");
+    return RKB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Certificate of each (ion, k) table from the row records, before or after the
+// contraction.  Rounding row a to the quantum h_a = 2^(e_a - bits) moves entry
+// (a, b) by about h_a |[X|Z]_b| + h_b |[X|Z]_a| (a random walk of K rounding
+// errors against the other row), so the Schwarz-relative error of the table
+// is estimated by
+//     est = max_a h_a / sqrt|R_aa|  *  max_b |[X|Z]_b| / sqrt|R_bb|
+// (rows with [X|Z] = 0 carry no rounding and are skipped; a vanishing or
+// non-finite diagonal gives est = inf).  Tables with est > limit are counted in
+// *flagged; the host recomputes them in FP64.  One block per table.
+namespace rkb {
+namespace split {
+__global__ void __launch_bounds__(256) certify_kernel(const long *__restrict__ grp_row0,
+                                                      const long *__restrict__ grp_n,
+                                                      const double *__restrict__ rowscale,
+                                                      const double *__restrict__ cbound, double limit,
+                                                      double *__restrict__ est, int *__restrict__ flagged) {
+    __shared__ double sm1[8], sm2[8];
+    __shared__ int sbad[8];
+    const long g = blockIdx.x;
+    const long row0 = grp_row0[g], n = grp_n[g];
+    double m1 = 0.0, m2 = 0.0;
+    bool bad = false;
+    for (long i = threadIdx.x; i < n; i += blockDim.x) {
+        const long r = row0 + i;
+        const double nrm = cbound[r * CB_STRIDE + 4];
+        if (nrm == 0.0) continue;
+        const double rd = sqrt(fabs(cbound[r * CB_STRIDE + 5]));
+        const double t1 = rowscale[r] / rd, t2 = nrm / rd;
+        if (!(t1 <= DBL_MAX) || !(t2 <= DBL_MAX)) {
+            bad = true;
+        } else {
+            m1 = fmax(m1, t1);
+            m2 = fmax(m2, t2);
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+        m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    const int badw = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+        sm1[wid] = m1;
+        sm2[wid] = m2;
+        sbad[wid] = badw;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool any = false;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            m1 = fmax(m1, sm1[w]);
+            m2 = fmax(m2, sm2[w]);
+            any |= sbad[w] != 0;
+        }
+        const double e = any ? INFINITY : m1 * m2;
+        est[g] = e;
+        if (!(e <= limit)) atomicAdd(flagged, 1);
+    }
+}
+}  // namespace split
+}  // namespace rkb
+
+extern "C" int rkb_split_certify(const long *d_grp_row0, const long *d_grp_n, long n_groups, const double *d_rowscale,
+                                 const double *d_cbound, double limit, double *d_est, int *d_flagged, void *stream) {
+    RKB_CHECK_ARG(n_groups >= 0 && n_groups <= 0x7fffffffL, "invalid group count %ld", n_groups);
+    RKB_CHECK_ARG(limit >= 0.0, "the certificate limit must be >= 0");
+    RKB_CHECK_ARG(d_flagged != nullptr && (n_groups == 0 || (d_grp_row0 && d_grp_n && d_rowscale && d_cbound && d_est)),
+                  "null argument");
+    cudaStream_t st = as_stream(stream);
+    RKB_CUDA(cudaMemsetAsync(d_flagged, 0, sizeof(int), st));
+    if (n_groups == 0) return RKB_OK;
+    certify_kernel<<<(unsigned)n_groups, 256, 0, st>>>(d_grp_row0, d_grp_n, d_rowscale, d_cbound, limit, d_est,
+                                                      d_flagged);
+    RKB_LAUNCHED("certify_kernel");
     return RKB_OK;
 }
 

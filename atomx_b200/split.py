@@ -28,7 +28,7 @@ import torch
 from . import _native
 from .split_plan import (bits_for_moduli, concat_tables, crt_constants, green_factor_packed, moduli_needed,
                          table_z_count)
-from .tables import IonDevice, tile_tasks
+from .tables import IonDevice, fp64_group_table, tile_tasks
 
 __all__ = ["SplitEngine", "IonRows", "factors_for_grid", "host_tables", "choose_width", "DEFAULT_BITS"]
 
@@ -40,6 +40,37 @@ DEFAULT_BITS = 36
 #: longest contraction the CRT kernel takes: its int32 accumulators are made
 #: nonnegative by a bias of m * 2^18 >= kdim * 128^2 for every modulus m >= 223
 KDIM_MAX = 3456
+
+
+#: doubles per row of the row record (screen bounds, |[X|Z]|, R_aa)
+CB_STRIDE = 8
+#: certificate limit: a table whose estimated Schwarz-relative split error
+#: exceeds this is recomputed in FP64.  The estimate tracks the measured error
+#: within a factor 0.7..3, so 2.5e-11 keeps every table below 1e-10.
+CERT_LIMIT = 2.5e-11
+
+
+def certify(grp_row0, grp_n, rowscale, cbound, limit: float, est, status, stream=None) -> None:
+    """Enqueue the per-table certificate: est[g] and status[1] = count over limit."""
+    L = _native.load()
+    _native.check(L.rkb_split_certify(grp_row0.data_ptr(), grp_n.data_ptr(), grp_n.numel(), rowscale.data_ptr(),
+                                      cbound.data_ptr(), float(limit), est.data_ptr(), status.data_ptr() + 4,
+                                      _native.stream_handle(stream)), "rkb_split_certify")
+
+
+def launch_stream(stream):
+    """The stream work was enqueued on (None means the current stream), waited
+    for so that its status words can be read."""
+    s = stream if stream is not None else torch.cuda.current_stream()
+    s.synchronize()
+    return s
+
+
+def join_stream(s) -> None:
+    """Make the current stream wait for work enqueued on ``s``."""
+    cur = torch.cuda.current_stream()
+    if s != cur:
+        cur.wait_stream(s)
 
 
 def check_kdim(kdim: int) -> None:
@@ -108,10 +139,9 @@ def host_tables(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
         koff[k] = offs[i]
         F = factors[k]
         u_ = F[:n].reshape(nv, ng).T
-        ell_ = F[n:2 * n].reshape(nv, ng).T
-        L_ = F[2 * n:2 * n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
-        C_ = F[2 * n + nv * ng * ng:2 * n + nv * ng * ng + n].reshape(nv, ng).T
-        t = np.concatenate([u_.ravel(), ell_.ravel(), C_.ravel(), L_.ravel()])
+        L_ = F[n:n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
+        C_ = F[n + nv * ng * ng:n + nv * ng * ng + n].reshape(nv, ng).T
+        t = np.concatenate([u_.ravel(), C_.ravel(), L_.ravel()])
         koff_t[k] = pos
         pos += t.shape[0]
         parts.append(t)
@@ -250,7 +280,7 @@ class IonRows:
         a_ptr = resA.data_ptr() + rb * kpad
         b_ptr = resB.data_ptr() + rb * kpad if resB is not None else 0
         rs, lf = rowscale.data_ptr() + 8 * rb, left.data_ptr() + 8 * rb * cwp
-        rt, cb = right.data_ptr() + 8 * rb * cwp, cbound.data_ptr() + 16 * rb
+        rt, cb = right.data_ptr() + 8 * rb * cwp, cbound.data_ptr() + 8 * CB_STRIDE * rb
         if self.kind == "cells":
             _native.check(L.rkb_split_rows_cells(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
                                                  dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
@@ -285,7 +315,7 @@ class SplitEngine:
 
     def __init__(self, dev: IonDevice, bits: int | None = None, tau: float = 1e-3, n_mod: int | None = None,
                  corr_floor: float | None = None, fused: bool | None = None, materialize: bool = True,
-                 rows_kernel: str | None = None):
+                 rows_kernel: str | None = None, cert_limit: float = CERT_LIMIT):
         _native.require_device()
         self.dev = dev
         plan = dev.plan
@@ -298,7 +328,7 @@ class SplitEngine:
         check_kdim(self.kpad)
         self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
-        self.cw = ng
+        self.cw = ng + 2  # g_0 and the two core-body coupling moments
         self.cwp = _round_up(self.cw, 2)
         nrows = plan.n_rows
         # rows padded to whole 128-row TMA boxes (zero rows never reach a stored entry)
@@ -309,7 +339,7 @@ class SplitEngine:
         self.rowscale = torch.empty(nrows, dtype=torch.float64, device=d)
         self.left = torch.empty((nrows, self.cwp), dtype=torch.float64, device=d)
         self.right = torch.empty_like(self.left)
-        self.cbound = torch.empty((nrows, 2), dtype=torch.float64, device=d)
+        self.cbound = torch.empty((nrows, CB_STRIDE), dtype=torch.float64, device=d)
         # scratch of the two-kernel path: the FP64 rows [X | Z] before rounding
         self.xwork = (torch.empty((nrows, self.kpad), dtype=torch.float64, device=d) if R.kind == "two" else None)
         #: skip the FP64 core correction of a block when its bound is below
@@ -331,7 +361,14 @@ class SplitEngine:
         bounds = np.searchsorted(tasks[:, 0], np.arange(len(sizes) + 1))
         self.task_range = [(int(bounds[i]), int(bounds[i + 1])) for i in range(len(sizes))]
         self.grp_out_zero = torch.zeros(len(sizes), dtype=torch.int64, device=d)
-        self.status = torch.zeros(1, dtype=torch.int32, device=d)
+        #: [contraction status, number of tables whose certificate failed]
+        self.status = torch.zeros(2, dtype=torch.int32, device=d)
+        #: certificate estimate of every multipole table (Schwarz-relative error)
+        self.est = torch.zeros(len(sizes), dtype=torch.float64, device=d)
+        self.cert_limit = float(cert_limit)
+        #: multipoles recomputed in FP64 by the last check_status()
+        self.escalated: list = []
+        self._stream = None
         #: the whole table (None when the engine only streams multipole tables)
         self.out = torch.empty(self.total, dtype=torch.float64, device=d) if materialize else None
         self._mod_c = (np.ctypeslib.as_ctypes(np.ascontiguousarray(self.moduli, dtype=np.int32)),
@@ -343,16 +380,21 @@ class SplitEngine:
 
     @property
     def launches_per_step(self) -> int:
-        return 3 if self.ion_rows.kind == "two" else 2
+        """Kernels per table run: the row kernel(s), the certificate, the contraction."""
+        return 4 if self.ion_rows.kind == "two" else 3
 
     def column_positions(self, k: int) -> np.ndarray:
         """Residue position of every column of the row [X | Z] of multipole k."""
         return self.ion_rows.column_positions(k)
 
     def rows(self, stream=None) -> None:
+        """Row kernels, then the certificate of every table (both async)."""
+        self._stream = stream
         self.ion_rows.launch(self.bits, self.n_mod, self._mod_c[0], self.resA, self.resB, self.kpad, 0,
                              self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp,
                              self.xwork, stream)
+        certify(self.grp_row0, self.grp_n, self.rowscale, self.cbound, self.cert_limit, self.est, self.status,
+                stream)
 
     def contract(self, stream=None) -> None:
         if self.out is None:
@@ -381,6 +423,11 @@ class SplitEngine:
         s = stream if stream is not None else torch.cuda.current_stream()
         plan = self.dev.plan
         self.rows(s)
+        # which tables go to FP64 is known from the rows alone: one wait here
+        with torch.cuda.stream(s):
+            flagged = int(self.status[1].item())
+        fp64 = set(self._failing(self.est.cpu().numpy())) if flagged else set()
+        self.escalated = sorted(fp64)
         nmax = max(plan.n_of_k(k) for k in plan.ks)
         bufs = [torch.empty(nmax * nmax, dtype=torch.float64, device=self.resA.device) for _ in range(2)]
         #: device bytes the engine holds while streaming (buffers included)
@@ -389,9 +436,13 @@ class SplitEngine:
             nk = plan.n_of_k(k)
             t0, t1 = self.task_range[gi]
             buf = bufs[gi % 2][:nk * nk]
-            self._contract(self.grp_out_zero, t0, t1, buf, s)
+            if k in fp64:
+                fp64_group_table(self.dev, k, buf, s)
+            else:
+                self._contract(self.grp_out_zero, t0, t1, buf, s)
             sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
         self._bufs = bufs  # kept alive until the caller has waited for the stream
+        self._streamed = True
         if check:
             self.check_status()
 
@@ -405,18 +456,37 @@ class SplitEngine:
     def device_bytes(self) -> int:
         """Bytes of the engine's own device buffers (not the ion's inputs)."""
         ts = [self.ktab, self.koff, self.resA, self.resB, self.rowscale, self.left, self.right, self.cbound,
-              self.xwork, self.zcount, self.tasks, self.out]
+              self.xwork, self.zcount, self.tasks, self.est, self.out]
         return int(sum(t.numel() * t.element_size() for t in ts if t is not None))
 
+    def _failing(self, est) -> list:
+        return [k for gi, k in enumerate(self.dev.plan.ks) if not est[gi] <= self.cert_limit]
+
     def check_status(self) -> None:
-        st = int(self.status.item())
+        """Wait for the device, raise a contraction error, and recompute in FP64
+        (on the launch stream) every table whose certificate failed; the
+        multipoles recomputed are listed in ``escalated``."""
+        s = launch_stream(self._stream)
+        st, flagged = self.status.tolist()
         if st:
-            self.status.zero_()
+            self.status[0] = 0
             _native.check(st, "crt_syrk_kernel")
+        if getattr(self, "_streamed", False):  # the stream path chose per table already
+            self._streamed = False
+            return
+        self.escalated = []
+        if flagged and self.out is not None:
+            for k in self._failing(self.est.cpu().numpy()):
+                nk = self.dev.plan.n_of_k(k)
+                o = self.offsets[k]
+                fp64_group_table(self.dev, k, self.out[o:o + nk * nk], s)
+                self.escalated.append(k)
+            join_stream(s)
 
     def info(self) -> dict:
         return {"bits": self.bits, "n_mod": self.n_mod, "moduli": [int(m) for m in self.moduli], "fused": self.fused,
-                "rows_kernel": self.ion_rows.kind,
+                "rows_kernel": self.ion_rows.kind, "cert_limit": self.cert_limit,
+                "fp64_multipoles": list(self.escalated),
                 "kpad": self.kpad, "z_columns": {int(k): v for k, v in self.nz.items()},
                 "device_bytes": self.device_bytes(),
                 "tasks": self.n_tasks}

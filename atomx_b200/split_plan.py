@@ -11,31 +11,42 @@ u = r^-(k+1), v = r^k.  Off-diagonal cell blocks are rank one, so G is
 block-semiseparable.
 
 Split G at cell 0 (the cell [0, r_min] whose partial rule acts on an
-endpoint-singular integrand and whose block is violently indefinite) and
-eliminate the body first, the core last:
+endpoint-singular integrand and whose block is violently indefinite) and keep
+the core in FP64:
 
   R = X_ac . X_bd - Z_ac . Z_bd + left_ac . right_bd
 
 * body (cells >= 1): a block Cholesky of the semiseparable G_bb computed by
   the recursion  S_m = D_m - sigma_m u_m u_m^T,  L_mm L_mm^T = S_m + Delta_m,
   c_m = L_mm^{-1} (v_m - sigma_m u_m),  sigma_{m+1} = sigma_m + |c_m|^2,
-  which gives X = L^T g per row in O(N ng):
+  which gives X = L^T g_b per row in O(N ng):
       X_m = L_mm^T g_m + c_m * sum_{m' > m} u_m'.g_m'.
   Delta_m (a modified-Cholesky shift, rank = number of Schur eigenvalues
   below tau * lambda_max of the diagonally scaled block) is returned as
   extra columns Z with a negative sign: g^T Delta g = sum_e (z_e . g_m)^2;
-* the core-body coupling G_cb = v_0 u_b^T is rank one and moves into X:
-  with ell = L^-1 u_b (block forward substitution,
-  L_mm ell_m = u_m (1 - sum_{m'<m} c_m'.ell_m')),
-      X = L^T g_b + ell * (v_0 . g_0),
-  which reproduces both cross terms (ell . L^T g = u_b . g);
-* what is left is the core Schur complement S_c = G_00 - |ell|^2 v_0 v_0^T,
-  kept in FP64: left = g_0, right = S_c g_0.  For physical densities it is
-  many orders below the entries (cell 0 holds almost no charge).
+* core (cell 0) and the core-body coupling G_cb = v_0 u_b^T stay in FP64:
+      left  = [g_0, alpha sx, q / sx],   right = [G_00 g_0, q / sx, alpha sx]
+  with alpha = v_0 . g_0 (the core multipole moment), q = u_b . g_b (the
+  body's potential moment at the origin), so left_ac . right_bd =
+  g0_ac^T G_00 g0_bd + alpha_ac q_bd + q_ac alpha_bd.  The scale
+  sx = r_b^-(k+1)/2 r_l^-k/2 (r_l the last core node, r_b the first body
+  node) bounds both |alpha sx| and |q / sx| by |g|_1 / sqrt(r_b).
 
-|X_ac.X_bd| <= |X_ac||X_bd| = sqrt(R_acac R_bdbd) (up to the small Delta),
-so a per-row fixed-point split of X has an error bounded relative to the
-Schwarz scale of every entry, which is what the split engine needs.
+Folding the coupling into X instead (X += ell alpha with ell = L^-1 u_b, the
+core Schur complement G_00 - |ell|^2 v_0 v_0^T left in FP64) is exact in
+real arithmetic but |ell|^2 ~ r_b^-(2k+1): on coarse grids (first body node
+near 1e-5, cell ratios ~60) the folded term exceeds R by up to 1e20 and
+cancels against the Schur complement, which no fixed-point split survives.
+Kept apart, alpha_ac q_bd is as small as the physics makes it.
+
+|X_ac.X_bd| <= |X_ac||X_bd| = sqrt(R_acac R_bdbd) (up to the small Delta and
+the core terms), so a per-row fixed-point split of X has an error bounded
+relative to the Schwarz scale of every entry, which is what the split engine
+needs.  Where the core block itself cancels most of the body energy (wide
+origin cells at mid k: g0^T G_00 g0 near -R_body), |X|^2 exceeds R_acac by
+the same factor and the split's error grows with it; the engines certify
+every multipole table from per-row norms and recompute the ones that fail in
+FP64.
 
 CRT constants
 -------------
@@ -150,14 +161,9 @@ def green_factor(r_flat: np.ndarray, ng: int, k: int, tau: float = 1e-3) -> dict
         Lb[m] = Lm
         C[m] = np.linalg.solve(Lm, v[m] - sigma * u[m])
         sigma += float(C[m] @ C[m])
-    ell = np.zeros((nv, ng))
-    s_acc = 0.0
-    for m in range(1, nv):
-        ell[m] = np.linalg.solve(Lb[m], u[m] * (1.0 - s_acc))
-        s_acc += float(C[m] @ ell[m])
-    Gcc = u[0][:, None] * v[0][None, :] * mo + v[0][:, None] * u[0][None, :] * mi
-    Sc = Gcc - float(np.sum(ell * ell)) * np.outer(v[0], v[0])
-    return dict(k=k, nv=nv, ng=ng, u=u, v0=v[0].copy(), Lb=Lb, C=C, Gcc=Gcc, ell=ell, Sc=Sc,
+    G00 = u[0][:, None] * v[0][None, :] * mo + v[0][:, None] * u[0][None, :] * mi
+    sx = float(np.sqrt(u[1, 0]) / np.sqrt(v[0, -1]))
+    return dict(k=k, nv=nv, ng=ng, u=u, v0=v[0].copy(), Lb=Lb, C=C, G00=G00, sx=sx,
                 zcell=np.asarray(zcell, dtype=np.int64), zvec=np.asarray(zvec).reshape(-1, ng))
 
 
@@ -171,7 +177,7 @@ def green_factor_packed(r_flat: np.ndarray, ng: int, k: int, tau: float = 1e-3) 
     mo, mi = yk_partial_matrices(ng)
     mo = np.ascontiguousarray(mo, dtype=np.float64)
     mi = np.ascontiguousarray(mi, dtype=np.float64)
-    cap = 2 * nv * ng + nv * ng * ng + nv * ng + ng + ng * ng + 1 + nv * ng * (ng + 1)
+    cap = nv * ng + nv * ng * ng + nv * ng + ng + ng * ng + 2 + nv * ng * (ng + 1)
     out = np.empty(cap, dtype=np.float64)
     got = L.rkb_green_factor(r.ctypes.data, nv, ng, int(k), float(tau), mo.ctypes.data, mi.ctypes.data,
                              out.ctypes.data, cap)
@@ -194,11 +200,12 @@ def concat_tables(tables: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray]:
 def factor_table_layout(nv: int, ng: int) -> dict:
     """Offsets (in doubles) of the pieces of one packed factor table."""
     n = nv * ng
-    o = {"u": 0, "ell": n, "Lb": 2 * n}
+    o = {"u": 0, "Lb": n}
     o["C"] = o["Lb"] + nv * ng * ng
     o["v0"] = o["C"] + nv * ng
-    o["Sc"] = o["v0"] + ng
-    o["nz"] = o["Sc"] + ng * ng
+    o["G00"] = o["v0"] + ng
+    o["sx"] = o["G00"] + ng * ng
+    o["nz"] = o["sx"] + 1
     o["z"] = o["nz"] + 1
     return o
 
@@ -206,17 +213,16 @@ def factor_table_layout(nv: int, ng: int) -> dict:
 def pack_factors(factors: list[dict]) -> tuple[np.ndarray, np.ndarray]:
     """Concatenate per-k factor tables: returns (flat doubles, offsets by list index).
 
-    Layout of one table (doubles): u[N] | ell[N] | Lb[nv][ng][ng] | C[nv][ng] |
-    v0[ng] | Sc[ng][ng] | nZ | nZ x (cell, z[ng]).
+    Layout of one table (doubles): u[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] |
+    G00[ng][ng] | sx | nZ | nZ x (cell, z[ng]).
     """
     parts, offs, off = [], [], 0
     for F in factors:
-        nv, ng = F["nv"], F["ng"]
         nz = F["zcell"].shape[0]
         z = np.concatenate([F["zcell"].astype(np.float64)[:, None], F["zvec"]], axis=1).ravel() if nz else \
             np.zeros(0)
-        t = np.concatenate([F["u"].ravel(), F["ell"].ravel(), F["Lb"].ravel(), F["C"].ravel(), F["v0"],
-                            F["Sc"].ravel(), [float(nz)], z])
+        t = np.concatenate([F["u"].ravel(), F["Lb"].ravel(), F["C"].ravel(), F["v0"], F["G00"].ravel(),
+                            [float(F["sx"]), float(nz)], z])
         offs.append(off)
         parts.append(t)
         off += t.shape[0]

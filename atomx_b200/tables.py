@@ -28,7 +28,8 @@ from .plan import TablePlan, make_plan
 from .yk import yk_partial_matrices
 
 __all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "upload_ion", "upload_values", "slater_rk_tables",
-           "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE"]
+           "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE",
+           "fp64_group_table"]
 
 TILE = 128
 
@@ -190,6 +191,36 @@ def run_fp64(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, stream=None) 
     _native.check(L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
                                             ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr(),
                                             ws.n_tasks, out.data_ptr(), s), "rkb_table_contract_fp64")
+
+
+def fp64_group_table(dev: IonDevice, k: int, out: torch.Tensor, stream=None) -> None:
+    """The plain FP64 table of one multipole of one ion into ``out`` (n_k * n_k
+    doubles on the device): the Y^k rows of that multipole's plan rows, then
+    one contraction.  The split engines use it for the tables whose
+    certificate fails."""
+    L = _native.load()
+    s = _native.stream_handle(stream)
+    plan = dev.plan
+    nk, r0 = plan.n_of_k(k), int(plan.k_row_offset[k])
+    if out.numel() < nk * nk:
+        raise ValueError(f"output holds {out.numel()} doubles; multipole {k} needs {nk * nk}")
+    ld = _round_up(dev.n, 32)
+    d = dev.Pv.device
+    g = torch.empty((nk, ld), dtype=torch.float64, device=d)
+    y = torch.empty_like(g)
+    _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                        dev.row_pair.data_ptr() + 8 * r0, dev.row_k.data_ptr() + 4 * r0, nk,
+                                        dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
+                                        dev.mi.data_ptr(), g.data_ptr(), y.data_ptr(), ld, s),
+                  "rkb_table_rows_fp64")
+    tasks = torch.as_tensor(tile_tasks([nk]).reshape(-1), device=d)
+    meta = torch.tensor([0, nk, 0], dtype=torch.int64, device=d)
+    _native.check(L.rkb_table_contract_fp64(g.data_ptr(), y.data_ptr(), ld, ld, meta.data_ptr(),
+                                            meta.data_ptr() + 8, meta.data_ptr() + 16, tasks.data_ptr(),
+                                            tasks.numel() // 3, out.data_ptr(), s), "rkb_table_contract_fp64")
+    # the temporaries return to the pool of the stream that used them
+    for t in (g, y, tasks, meta):
+        t.record_stream(stream if stream is not None else torch.cuda.current_stream())
 
 
 def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, sink=None,

@@ -322,7 +322,9 @@ def run_gpu(args):
         eng = SplitEngine(dev)
 
         def step():
-            return eng.run(stream=stream, upload=False, check=False)
+            # check=True: the per-table certificate is read back every step and
+            # any table that fails it is recomputed in FP64 inside the step
+            return eng.run(stream=stream, upload=False, check=True)
 
         launches_per_step = eng.launches_per_step
     else:
@@ -387,6 +389,8 @@ def run_gpu(args):
         line["serve"] = serve_leg(args)
     if not args.no_grid and engine == "split":
         line["grid_yk"] = grid_leg()
+    if not args.no_batch and engine == "split":
+        line["batch"] = batch_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
@@ -549,6 +553,61 @@ def grid_leg(rows: int = 4000, n: int = 20000, reps: int = 5) -> dict:
             "algorithmic_gbs": bytes_row * rows / (ms / 1e3) / 1e9}
 
 
+def batch_leg(reps: int = 3) -> dict:
+    """The 64-ion uneven batch (Z 20..83, 40..160 B-splines of order 7 or 9,
+    20..150 spinors, k_max = 12): every table of every ion in one persistent
+    contraction launch, captured with the row launches and the certificate as
+    one CUDA graph.  A replay is timed with its certificate readback and the
+    FP64 recomputation of the tables that fail it; the split width and task
+    order come from the autotuner under the FP64 error gate."""
+    import torch
+
+    from atomx_b200 import autotune
+    from atomx_b200 import workloads as W
+    from atomx_b200.batch import Fp64Batch, SplitBatch
+    from atomx_b200.tables import upload_ion
+    devs = [upload_ion(W.build_ion(spec)) for spec in W.uneven_batch()]
+    entries = sum(d.plan.ordered_entries for d in devs)
+    s = torch.cuda.current_stream()
+
+    def timed(batch):
+        batch.capture()
+        batch.replay()
+        batch.check_status()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            batch.replay()
+            batch.check_status()
+            e1.record(s)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    fp = Fp64Batch(devs)
+    ms64 = timed(fp)
+    t0 = time.perf_counter()
+    tune = autotune.autotune_split_batch(devs, bits_choices=(36, 38), orders=("lpt", "group"), layouts=(None,),
+                                         ref=fp)
+    tune_s = time.perf_counter() - t0
+    del fp
+    torch.cuda.empty_cache()
+    sb = SplitBatch(devs, **tune.options())
+    ms = timed(sb)
+    info = sb.info()
+    return {"workload": "uneven batch: 64 ions (Z 20..83, ns 40..160, order 7/9, 20..150 spinors, k_max=12)",
+            "entries": entries, "split_ms": ms, "split_integrals_per_s": entries / (ms / 1e3),
+            "fp64_ms": ms64, "fp64_integrals_per_s": entries / (ms64 / 1e3), "speedup_split_vs_fp64": ms64 / ms,
+            "launches_per_replay": sb.launches_per_step, "graph": "one CUDA graph per engine",
+            "tables": len(sb.group_of), "fp64_tables": len(info["fp64_tables"]),
+            "autotune": {"chosen": tune.options(), "error_vs_fp64": tune.error, "tune_s": tune_s,
+                         "trials": [{k_: t[k_] for k_ in ("bits", "n_mod", "order", "ms", "error", "ok")}
+                                    for t in tune.trials]},
+            "split": {k_: info[k_] for k_ in ("bits", "n_mod", "kpad", "tasks", "rows", "row_kernels")}}
+
+
 def torch_sync():
     import torch
     torch.cuda.synchronize()
@@ -567,6 +626,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
     ap.add_argument("--serve", type=int, default=32, help="requests in the serving leg (0 = skip)")
     ap.add_argument("--no-grid", action="store_true", help="skip the arbitrary-grid Y^k leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-ion batch leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -165,22 +165,26 @@ int rkb_table_contract_fp64_groups(const double *d_g, const double *d_y, long ld
  * With g = w*rho, atomx's R^k(ac;bd) = g_ac^T G g_bd (numerics/yk.py:88 and
  * numerics/bspline/slater.py:130).  The engine writes
  *     R = X_ac.X_bd - Z_ac.Z_bd + left_ac.right_bd
- * with X, Z from a block Cholesky of the body of G (cells >= 1) including the
- * rank-one core-body coupling, and left/right the FP64 core (cell 0) Schur
- * complement terms.
+ * with X, Z from a block Cholesky of the body of G (cells >= 1), and
+ * left/right the FP64 terms of the core cell 0 and its rank-one coupling to
+ * the body: left = [g_0, alpha sx, q/sx, 0...], right = [G_00 g_0, q/sx,
+ * alpha sx, 0...] with alpha = v_0.g_0, q = u_b.g_b and the per-(grid, k)
+ * scale sx of the factor table.
  *
  * rkb_split_rows: per plan row q (pair d_row_pair[q], multipole d_row_k[q])
  * compute [X | Z], scale by 2^(bits - e_q) so |x| < 2^bits, round, and write
  * int8 residues x mod moduli[i] to d_resA[i][row_base+q][0..kpad) (d_resB, if
  * not NULL, gets the same with Z negated), 2^(e_q - bits) to d_rowscale, the
- * core correction vectors (width cwp >= ng) left = g_0, right = S_c g_0 to
- * d_left / d_right, and to d_cbound[2q], d_cbound[2q+1] the norms |g_0| and
- * |S_c g_0| divided by 2^e_q (>= the row maximum of |[X | Z]|).  d_ktab holds the
- * per-k factor tables at offsets d_koff[k] (layout in atomx_b200/split_plan.py)
- * and d_zcount[k] their Z-column counts.  d_xwork is caller-provided scratch
- * of (row_base + nrows) x kpad doubles that receives the FP64 rows [X | Z | 0]
- * before they are rounded.  A row with a non-finite value gets a NaN scale
- * and zero residues, so every entry it reaches comes out NaN.
+ * core vectors (width cwp >= ng + 2) to d_left / d_right, and the row record
+ * d_cbound[8q .. 8q+7]: |g_0|, |G_00 g_0|, |alpha sx|, |q/sx| divided by 2^e_q
+ * (>= the row maximum of |[X | Z]|; the contraction's correction screen),
+ * |[X | Z]| and the FP64 diagonal R_qq = |X|^2 - |Z|^2 + left.right (the
+ * certificate's inputs), 0, 0.  d_ktab holds the per-k factor tables at
+ * offsets d_koff[k] (layout at rkb_green_factor) and d_zcount[k] their
+ * Z-column counts.  d_xwork is caller-provided scratch of (row_base + nrows)
+ * x kpad doubles that receives the FP64 rows [X | Z | 0] before they are
+ * rounded.  A row with a non-finite value gets a NaN scale and zero residues,
+ * so every entry it reaches comes out NaN.
  * `moduli` is a HOST array of n_mod pairwise-coprime ints <= 256.
  *
  * rkb_split_contract: for every task (group, tile_i, tile_j >= tile_i) the
@@ -229,7 +233,7 @@ int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long orb_ld, co
  * ((m-1)*ng + node, then Z), positions from (nv-1)*ng + nZ up to kpad
  * written as zeros.  Besides the packed tables (d_ktab/d_koff) it reads a
  * cell-minor copy of each multipole's factors at d_ktab_t + d_koff_t[k]:
- * u[ng][nv] | ell[ng][nv] | C[ng][nv] | L[ng][ng][nv] (L[i][node][cell]).
+ * u[ng][nv] | C[ng][nv] | L[ng][ng][nv] (L[i][node][cell]).
  * Scales, core vectors and bounds as rkb_split_rows. */
 int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long orb_ld, const long *d_pairs,
                          const long *d_row_pair, const int *d_row_k, long nrows, const double *d_w,
@@ -243,8 +247,9 @@ int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long orb_ld, co
  * multipole k on the grid r (nv cells x ng nodes, mo/mi the ng x ng partial
  * matrices of atomx numerics/yk.py:65 yk_partial_matrices) with eigenvalue
  * shift threshold tau, in the layout rkb_split_rows reads (d_ktab):
- * u[N] | ell[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] | Sc[ng][ng] | nZ |
- * nZ x (cell, z[ng]).  Writes at most cap doubles to out; returns the count
+ * u[N] | Lb[nv][ng][ng] | C[nv][ng] | v0[ng] | G00[ng][ng] | sx | nZ |
+ * nZ x (cell, z[ng]), sx = r_b^-(k+1)/2 r_l^-k/2 (r_l the last core node,
+ * r_b the first body node).  Writes at most cap doubles to out; returns the count
  * written or a negative rkb_status.  atomx has no counterpart (its Y^k is
  * a scan, numerics/yk.py:88; this factors the same operator). */
 long rkb_green_factor(const double *r, int nv, int ng, int k, double tau, const double *mo,
@@ -263,6 +268,18 @@ int rkb_split_contract(const signed char *d_resA, const signed char *d_resB, lon
                        const long *d_grp_row0, const long *d_grp_n, const long *d_grp_kdim,
                        const long *d_grp_out, const int *d_tasks, long n_tasks, double *d_out,
                        int *d_status, void *stream);
+
+/* rkb_split_certify: per table g (rows d_grp_row0[g] .. + d_grp_n[g]) the
+ * estimate d_est[g] = max_a h_a / sqrt|R_aa| * max_b |[X|Z]_b| / sqrt|R_bb|
+ * of the split's Schwarz-relative error from the row records (h = d_rowscale,
+ * rows with [X|Z] = 0 skipped, a vanishing or non-finite diagonal gives inf);
+ * *d_flagged (device int, cleared by the call) counts the tables with
+ * d_est[g] > limit.  Only the row kernels' output is read, so it may run
+ * before or after rkb_split_contract.  atomx has no counterpart: it computes
+ * every entry in FP64; the split engine recomputes the flagged tables with
+ * the FP64 entry points. */
+int rkb_split_certify(const long *d_grp_row0, const long *d_grp_n, long n_groups, const double *d_rowscale,
+                      const double *d_cbound, double limit, double *d_est, int *d_flagged, void *stream);
 
 /* ---------------------------------------------------------------------------
  * rkb_split_rows_noalloc: no counterpart in the reference (an addition of this

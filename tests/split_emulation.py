@@ -19,14 +19,17 @@ def unpack_table(flat, off, nv, ng):
     t = flat[off:]
     nz = int(t[o["nz"]])
     z = t[o["z"]:o["z"] + nz * (ng + 1)].reshape(nz, ng + 1) if nz else np.zeros((0, ng + 1))
-    return dict(u=t[:n].reshape(nv, ng), ell=t[o["ell"]:o["ell"] + n].reshape(nv, ng),
-                Lb=t[o["Lb"]:o["Lb"] + nv * ng * ng].reshape(nv, ng, ng),
+    return dict(u=t[:n].reshape(nv, ng), Lb=t[o["Lb"]:o["Lb"] + nv * ng * ng].reshape(nv, ng, ng),
                 C=t[o["C"]:o["C"] + nv * ng].reshape(nv, ng), v0=t[o["v0"]:o["v0"] + ng],
-                Sc=t[o["Sc"]:o["Sc"] + ng * ng].reshape(ng, ng), zcell=z[:, 0].astype(int), zvec=z[:, 1:])
+                G00=t[o["G00"]:o["G00"] + ng * ng].reshape(ng, ng), sx=float(t[o["sx"]]),
+                zcell=z[:, 0].astype(int), zvec=z[:, 1:])
 
 
 def transform_rows(g, F, nv, ng):
-    """[X | Z], left, right for rows g (rows, N) with one factor table F."""
+    """[X | Z], left, right for rows g (rows, N) with one factor table F.
+
+    left = [g_0, alpha sx, q / sx], right = [G_00 g_0, q / sx, alpha sx] with
+    alpha = v_0 . g_0 and q = u_b . g_b (the suffix sum at cell 0)."""
     rows = g.shape[0]
     gb = g.reshape(rows, nv, ng)
     d = np.einsum("qmi,mi->qm", gb, F["u"])
@@ -35,12 +38,14 @@ def transform_rows(g, F, nv, ng):
     tn = np.concatenate([suf[:, 1:], np.zeros((rows, 1))], axis=1)
     g0 = gb[:, 0, :]
     alpha = g0 @ F["v0"]
-    X = np.einsum("mij,qmi->qmj", F["Lb"], gb) + F["C"][None] * tn[:, :, None] + F["ell"][None] * alpha[:, None, None]
+    q = tn[:, 0]
+    X = np.einsum("mij,qmi->qmj", F["Lb"], gb) + F["C"][None] * tn[:, :, None]
     X = X[:, 1:, :].reshape(rows, -1)
     Z = np.stack([gb[:, m, :] @ z for m, z in zip(F["zcell"], F["zvec"])], axis=1) if len(F["zcell"]) else \
         np.zeros((rows, 0))
-    left = g0
-    right = g0 @ F["Sc"].T
+    sx = F["sx"]
+    left = np.concatenate([g0, (alpha * sx)[:, None], (q / sx)[:, None]], axis=1)
+    right = np.concatenate([g0 @ F["G00"].T, (q / sx)[:, None], (alpha * sx)[:, None]], axis=1)
     return X, Z, left, right
 
 

@@ -98,8 +98,13 @@ def test_autotuner_meets_gate_and_caches(batch8):
     res = autotune.autotune_split_batch(devs4, **opts)
     assert res.error <= 0.5 * GATE and not res.cached
     assert len(res.trials) == 4 and all(t["ms"] > 0 for t in res.trials)
-    # 32 bits are too few for the gate's margin on these ions; 38 pass
-    assert not any(t["ok"] for t in res.trials if t["bits"] == 32)
-    assert all(t["ok"] for t in res.trials if t["bits"] == 38) and res.bits == 38
+    # 32 bits are too few for these ions: their tables fail the certificate and
+    # are recomputed in FP64, which keeps every candidate within the gate but
+    # costs the narrow split its speed; 38 bits keep the tables on the split path
+    t32 = [t for t in res.trials if t["bits"] == 32]
+    t38 = [t for t in res.trials if t["bits"] == 38]
+    assert all(t["ok"] for t in res.trials)
+    assert min(t["fp64_tables"] for t in t32) > max(t["fp64_tables"] for t in t38)
+    assert res.bits == 38
     again = autotune.autotune_split_batch(devs4, **opts)
     assert again.cached and again.options() == res.options()

@@ -75,10 +75,19 @@ def test_rows_kernel_matches_cpu_transform(name, rows_kernel):
         assert np.all(np.abs(got - ref) <= (0.5 + 1e-6) * rs[rows][:, None] + 1e-15 * np.abs(ref)), k
         unused = np.setdiff1d(np.arange(eng.kpad), pos)
         assert np.all(resA[:, rows][:, :, unused] == 0)
-        lsc = np.abs(lf).max(axis=1, keepdims=True) + 1e-300
-        assert np.all(np.abs(left[rows] - lf) <= 1e-13 * lsc), k
-        sc = np.abs(rt).max(axis=1, keepdims=True) + 1e-300
-        assert np.all(np.abs(right[rows] - rt) <= 1e-12 * sc), k
+        # core columns relative to the row's largest; the two coupling moments
+        # (sums with cancellation, summed in another order on the device)
+        # relative to the sums of their terms' magnitudes
+        gb = g.reshape(-1, nv, ng)
+        a_abs = np.abs(gb[:, 0] * F["v0"]).sum(axis=1) * F["sx"]
+        q_abs = np.abs(gb[:, 1:] * F["u"][1:]).sum(axis=(1, 2)) / F["sx"]
+        mom = np.stack([a_abs, q_abs], axis=1)
+        lsc = np.abs(lf[:, :ng]).max(axis=1, keepdims=True) + 1e-300
+        assert np.all(np.abs(left[rows, :ng] - lf[:, :ng]) <= 1e-13 * lsc), k
+        sc = np.abs(rt[:, :ng]).max(axis=1, keepdims=True) + 1e-300
+        assert np.all(np.abs(right[rows, :ng] - rt[:, :ng]) <= 1e-12 * sc), k
+        assert np.all(np.abs(left[rows, ng:] - lf[:, ng:]) <= 1e-13 * mom), k
+        assert np.all(np.abs(right[rows, ng:] - rt[:, ng:]) <= 1e-13 * mom[:, ::-1]), k
         if eng.resB is not None:
             resB = eng.resB.cpu().numpy().astype(np.int64)
             zpos, bpos = pos[X.shape[1]:], pos[:X.shape[1]]
@@ -205,20 +214,31 @@ def test_split_table_large_ions(name):
 
 
 def test_split_bits_control_error():
-    """More bits, smaller error (the error model is ~2^-bits of the Schwarz scale)."""
+    """More bits, smaller error (the error model is ~2^-bits of the Schwarz
+    scale), measured with the certificate off; with it on, the tables of the
+    narrow splits fail their certificate and come back from the FP64 engine."""
     from atomx_b200 import workloads as W
     from atomx_b200.tables import slater_rk_tables_from_values, tables_for, upload_values
     ion = W.build_ion(W.neon_small())
     Pg, Qg = _values(ion)
     bd = ion.bsp
     plain = tables_for(upload_values(Pg, Qg, ion.kappa, bd["gr"], bd["grw"], 2), "fp64")
-    errs = []
-    for bits in (20, 28, 36):
-        t = slater_rk_tables_from_values(Pg, Qg, ion.kappa, bd["gr"], bd["grw"], 2, precision="split", bits=bits)
+
+    def worst(t):
         e = 0.0
         for k in t.ks:
             A, B = t.table(k), plain.table(k)
             d = torch.sqrt(torch.outer(torch.diagonal(B).abs(), torch.diagonal(B).abs()))
             e = max(e, float(((A - B).abs() / d).max()))
-        errs.append(e)
+        return e
+
+    errs, est = [], []
+    for bits in (20, 28, 36):
+        t = slater_rk_tables_from_values(Pg, Qg, ion.kappa, bd["gr"], bd["grw"], 2, precision="split", bits=bits,
+                                         cert_limit=float("inf"))
+        assert t.info["fp64_multipoles"] == []
+        errs.append(worst(t))
     assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-10, errs
+    for bits in (20, 28):
+        t = slater_rk_tables_from_values(Pg, Qg, ion.kappa, bd["gr"], bd["grw"], 2, precision="split", bits=bits)
+        assert t.info["fp64_multipoles"] == list(t.ks) and worst(t) <= 1e-14

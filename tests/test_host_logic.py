@@ -58,13 +58,12 @@ def test_cell_minor_tables_are_transposes_of_the_packed_ones():
     for k in (0, 1, 2):
         F = H["flat"][H["koff"][k]:]
         T = H["flat_t"][H["koff_t"][k]:]
-        u, ell = F[:n].reshape(nv, ng), F[o["ell"]:o["ell"] + n].reshape(nv, ng)
+        u = F[:n].reshape(nv, ng)
         L = F[o["Lb"]:o["Lb"] + nv * ng * ng].reshape(nv, ng, ng)
         C = F[o["C"]:o["C"] + n].reshape(nv, ng)
         np.testing.assert_array_equal(T[:n].reshape(ng, nv), u.T)
-        np.testing.assert_array_equal(T[n:2 * n].reshape(ng, nv), ell.T)
-        np.testing.assert_array_equal(T[2 * n:3 * n].reshape(ng, nv), C.T)
-        np.testing.assert_array_equal(T[3 * n:3 * n + nv * ng * ng].reshape(ng, ng, nv), L.transpose(1, 2, 0))
+        np.testing.assert_array_equal(T[n:2 * n].reshape(ng, nv), C.T)
+        np.testing.assert_array_equal(T[2 * n:2 * n + nv * ng * ng].reshape(ng, ng, nv), L.transpose(1, 2, 0))
     assert host_tables(gr.ravel(), ng, [0, 1, 2]) is H  # cached
 
 

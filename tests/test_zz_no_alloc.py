@@ -18,6 +18,8 @@ pytestmark = pytest.mark.gpu
 
 #: RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES in include/rkb200.h (16 MiB of doubles)
 CAP = 2 * 1024 * 1024
+#: doubles per row of the row record (d_cbound)
+CB_STRIDE = 8
 
 
 def _outputs(torch, eng, nr):
@@ -27,7 +29,7 @@ def _outputs(torch, eng, nr):
     return dict(resA=res_a, resB=res_b, rowscale=torch.empty(nr, dtype=torch.float64, device=d),
                 left=torch.empty((nr, eng.cwp), dtype=torch.float64, device=d),
                 right=torch.empty((nr, eng.cwp), dtype=torch.float64, device=d),
-                cbound=torch.empty((nr, 2), dtype=torch.float64, device=d))
+                cbound=torch.empty((nr, CB_STRIDE), dtype=torch.float64, device=d))
 
 
 def _call(torch, eng, r0, nr, noalloc):
