@@ -33,9 +33,9 @@ import torch
 
 from . import _native
 from .split import (CB_STRIDE, CERT_LIMIT, IonRows, _round_up, certify, check_kdim, choose_width, join_stream,
-                    launch_stream)
+                    read_status)
 from .split_plan import crt_constants
-from .tables import TILE, IonDevice, RkTables, fp64_group_table, tile_tasks
+from .tables import TILE, Fp64Recompute, IonDevice, RkTables, tile_tasks
 
 __all__ = ["SplitBatch", "Fp64Batch", "batch_tasks"]
 
@@ -183,18 +183,19 @@ class SplitBatch(_Graphable):
     def check_status(self) -> None:
         """Wait for the device, raise a contraction error, and recompute in FP64
         every (ion, k) table whose certificate failed (listed in ``escalated``)."""
-        s = launch_stream(self._stream)
-        st, flagged = self.status.tolist()
+        s, (st, flagged) = read_status(self.status, self._stream)
         if st:
             self.status[0] = 0
             _native.check(st, "crt_syrk_kernel")
         self.escalated = []
         if flagged:
             est = self.est.cpu().numpy()
-            for j, (i, k) in enumerate(self.group_of):
-                if not est[j] <= self.cert_limit:
-                    fp64_group_table(self.devs[i], k, self.table(i, k).reshape(-1), s)
-                    self.escalated.append((i, k))
+            self.escalated = [gk for j, gk in enumerate(self.group_of) if not est[j] <= self.cert_limit]
+            key = tuple(self.escalated)
+            cache = self.__dict__.setdefault("_recompute_cache", {})
+            if key not in cache:
+                cache[key] = Fp64Recompute([(self.devs[i], k, self.offsets[(i, k)]) for i, k in key])
+            cache[key].run(self.out, s)
             join_stream(s)
 
     def table(self, ion: int, k: int) -> torch.Tensor:

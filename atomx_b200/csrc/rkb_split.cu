@@ -1416,16 +1416,18 @@ extern "C" int rkb_split_contract(const signed char *d_resA, const signed char *
 //     est = max_a h_a / sqrt|R_aa|  *  max_b |[X|Z]_b| / sqrt|R_bb|
 // (rows with [X|Z] = 0 carry no rounding and are skipped; a vanishing or
 // non-finite diagonal gives est = inf).  Tables with est > limit are counted in
-// *flagged; the host recomputes them in FP64.  One block per table.
+// *flagged; the host recomputes them in FP64.  One 1024-thread block per table.
 namespace rkb {
 namespace split {
-__global__ void __launch_bounds__(256) certify_kernel(const long *__restrict__ grp_row0,
+constexpr int CERT_THREADS = 1024;
+
+__global__ void __launch_bounds__(CERT_THREADS) certify_kernel(const long *__restrict__ grp_row0,
                                                       const long *__restrict__ grp_n,
                                                       const double *__restrict__ rowscale,
                                                       const double *__restrict__ cbound, double limit,
                                                       double *__restrict__ est, int *__restrict__ flagged) {
-    __shared__ double sm1[8], sm2[8];
-    __shared__ int sbad[8];
+    __shared__ double sm1[CERT_THREADS / 32], sm2[CERT_THREADS / 32];
+    __shared__ int sbad[CERT_THREADS / 32];
     const long g = blockIdx.x;
     const long row0 = grp_row0[g], n = grp_n[g];
     double m1 = 0.0, m2 = 0.0;
@@ -1480,8 +1482,8 @@ extern "C" int rkb_split_certify(const long *d_grp_row0, const long *d_grp_n, lo
     cudaStream_t st = as_stream(stream);
     RKB_CUDA(cudaMemsetAsync(d_flagged, 0, sizeof(int), st));
     if (n_groups == 0) return RKB_OK;
-    certify_kernel<<<(unsigned)n_groups, 256, 0, st>>>(d_grp_row0, d_grp_n, d_rowscale, d_cbound, limit, d_est,
-                                                      d_flagged);
+    certify_kernel<<<(unsigned)n_groups, CERT_THREADS, 0, st>>>(d_grp_row0, d_grp_n, d_rowscale, d_cbound, limit,
+                                                               d_est, d_flagged);
     RKB_LAUNCHED("certify_kernel");
     return RKB_OK;
 }

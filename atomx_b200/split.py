@@ -28,7 +28,7 @@ import torch
 from . import _native
 from .split_plan import (bits_for_moduli, concat_tables, crt_constants, green_factor_packed, moduli_needed,
                          table_z_count)
-from .tables import IonDevice, fp64_group_table, tile_tasks
+from .tables import Fp64Recompute, IonDevice, tile_tasks
 
 __all__ = ["SplitEngine", "IonRows", "factors_for_grid", "host_tables", "choose_width", "DEFAULT_BITS"]
 
@@ -58,12 +58,16 @@ def certify(grp_row0, grp_n, rowscale, cbound, limit: float, est, status, stream
                                       _native.stream_handle(stream)), "rkb_split_certify")
 
 
-def launch_stream(stream):
-    """The stream work was enqueued on (None means the current stream), waited
-    for so that its status words can be read."""
+def read_status(status, stream):
+    """Copy the device status words to pinned host memory on the stream the
+    work was enqueued on (None: the current stream) and wait for it: one
+    synchronisation.  Returns (stream, [words])."""
     s = stream if stream is not None else torch.cuda.current_stream()
+    host = torch.empty(status.shape, dtype=status.dtype, pin_memory=True)
+    with torch.cuda.stream(s):
+        host.copy_(status, non_blocking=True)
     s.synchronize()
-    return s
+    return s, host.tolist()
 
 
 def join_stream(s) -> None:
@@ -437,7 +441,7 @@ class SplitEngine:
             t0, t1 = self.task_range[gi]
             buf = bufs[gi % 2][:nk * nk]
             if k in fp64:
-                fp64_group_table(self.dev, k, buf, s)
+                self._recompute(((k, 0),)).run(buf, s)
             else:
                 self._contract(self.grp_out_zero, t0, t1, buf, s)
             sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
@@ -466,8 +470,7 @@ class SplitEngine:
         """Wait for the device, raise a contraction error, and recompute in FP64
         (on the launch stream) every table whose certificate failed; the
         multipoles recomputed are listed in ``escalated``."""
-        s = launch_stream(self._stream)
-        st, flagged = self.status.tolist()
+        s, (st, flagged) = read_status(self.status, self._stream)
         if st:
             self.status[0] = 0
             _native.check(st, "crt_syrk_kernel")
@@ -476,12 +479,17 @@ class SplitEngine:
             return
         self.escalated = []
         if flagged and self.out is not None:
-            for k in self._failing(self.est.cpu().numpy()):
-                nk = self.dev.plan.n_of_k(k)
-                o = self.offsets[k]
-                fp64_group_table(self.dev, k, self.out[o:o + nk * nk], s)
-                self.escalated.append(k)
+            self.escalated = self._failing(self.est.cpu().numpy())
+            self._recompute(tuple((k, self.offsets[k]) for k in self.escalated)).run(self.out, s)
             join_stream(s)
+
+    def _recompute(self, key) -> Fp64Recompute:
+        """FP64 recomputation plan for (k, output offset) groups, cached."""
+        cache = self.__dict__.setdefault("_recompute_cache", {})
+        plan = cache.get(key)
+        if plan is None:
+            plan = cache[key] = Fp64Recompute([(self.dev, k, o) for k, o in key])
+        return plan
 
     def info(self) -> dict:
         return {"bits": self.bits, "n_mod": self.n_mod, "moduli": [int(m) for m in self.moduli], "fused": self.fused,

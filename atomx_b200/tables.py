@@ -29,7 +29,7 @@ from .yk import yk_partial_matrices
 
 __all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "upload_ion", "upload_values", "slater_rk_tables",
            "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE",
-           "fp64_group_table"]
+           "Fp64Recompute"]
 
 TILE = 128
 
@@ -193,34 +193,49 @@ def run_fp64(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, stream=None) 
                                             ws.n_tasks, out.data_ptr(), s), "rkb_table_contract_fp64")
 
 
-def fp64_group_table(dev: IonDevice, k: int, out: torch.Tensor, stream=None) -> None:
-    """The plain FP64 table of one multipole of one ion into ``out`` (n_k * n_k
-    doubles on the device): the Y^k rows of that multipole's plan rows, then
-    one contraction.  The split engines use it for the tables whose
-    certificate fails."""
-    L = _native.load()
-    s = _native.stream_handle(stream)
-    plan = dev.plan
-    nk, r0 = plan.n_of_k(k), int(plan.k_row_offset[k])
-    if out.numel() < nk * nk:
-        raise ValueError(f"output holds {out.numel()} doubles; multipole {k} needs {nk * nk}")
-    ld = _round_up(dev.n, 32)
-    d = dev.Pv.device
-    g = torch.empty((nk, ld), dtype=torch.float64, device=d)
-    y = torch.empty_like(g)
-    _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
-                                        dev.row_pair.data_ptr() + 8 * r0, dev.row_k.data_ptr() + 4 * r0, nk,
-                                        dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
-                                        dev.mi.data_ptr(), g.data_ptr(), y.data_ptr(), ld, s),
-                  "rkb_table_rows_fp64")
-    tasks = torch.as_tensor(tile_tasks([nk]).reshape(-1), device=d)
-    meta = torch.tensor([0, nk, 0], dtype=torch.int64, device=d)
-    _native.check(L.rkb_table_contract_fp64(g.data_ptr(), y.data_ptr(), ld, ld, meta.data_ptr(),
-                                            meta.data_ptr() + 8, meta.data_ptr() + 16, tasks.data_ptr(),
-                                            tasks.numel() // 3, out.data_ptr(), s), "rkb_table_contract_fp64")
-    # the temporaries return to the pool of the stream that used them
-    for t in (g, y, tasks, meta):
-        t.record_stream(stream if stream is not None else torch.cuda.current_stream())
+class Fp64Recompute:
+    """Plain FP64 tables for a set of (ion, k) groups, written at given
+    offsets of an output buffer: one Y^k-rows launch per group into a shared
+    workspace, then one grouped persistent contraction over all of them.
+    The split engines use it for the tables whose certificate fails; the plan
+    (workspace, group and task lists) is built once and reused."""
+
+    def __init__(self, items):
+        """items: [(IonDevice, k, output offset in doubles)]."""
+        from .batch import batch_tasks
+        self.items = list(items)
+        d = self.items[0][0].Pv.device
+        self.ld = _round_up(max(dev.n for dev, _, _ in self.items), 32)
+        sizes = [dev.plan.n_of_k(k) for dev, k, _ in self.items]
+        kdims = [_round_up(dev.n, 16) for dev, _, _ in self.items]
+        self.row0 = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        self.max_kdim = max(kdims)
+        self.g = torch.empty((max(int(self.row0[-1]), 1), self.ld), dtype=torch.float64, device=d)
+        self.y = torch.empty_like(self.g)
+        meta = np.stack([self.row0[:-1], np.asarray(sizes, dtype=np.int64), np.asarray(kdims, dtype=np.int64),
+                         np.asarray([o for _, _, o in self.items], dtype=np.int64)])
+        self.meta = torch.as_tensor(meta, device=d)
+        tasks = batch_tasks(sizes, kdims, "lpt")
+        self.n_tasks = int(tasks.shape[0])
+        self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
+
+    def run(self, out: torch.Tensor, stream=None) -> None:
+        L = _native.load()
+        s = _native.stream_handle(stream)
+        for j, (dev, k, _) in enumerate(self.items):
+            r0 = int(dev.plan.k_row_offset[k])
+            off = int(self.row0[j]) * self.ld * 8
+            _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                                dev.row_pair.data_ptr() + 8 * r0, dev.row_k.data_ptr() + 4 * r0,
+                                                dev.plan.n_of_k(k), dev.r.data_ptr(), dev.w.data_ptr(), dev.nv,
+                                                dev.ng, dev.mo.data_ptr(), dev.mi.data_ptr(),
+                                                self.g.data_ptr() + off, self.y.data_ptr() + off, self.ld, s),
+                          "rkb_table_rows_fp64")
+        m = self.meta
+        _native.check(L.rkb_table_contract_fp64_groups(self.g.data_ptr(), self.y.data_ptr(), self.ld, self.max_kdim,
+                                                       m[2].data_ptr(), m[0].data_ptr(), m[1].data_ptr(),
+                                                       m[3].data_ptr(), self.tasks.data_ptr(), self.n_tasks,
+                                                       out.data_ptr(), s), "rkb_table_contract_fp64_groups")
 
 
 def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, sink=None,
