@@ -46,6 +46,8 @@ _SIGNATURES = {
     "rkb_split_fused_body_width": [_i, _i],
     "rkb_green_factor": [_vp, _i, _i, _i, _d, _vp, _vp, _vp, _l],
     "rkb_split_certify": [_vp, _vp, _l, _vp, _vp, _d, _vp, _vp, _vp],
+    "rkb_occupied_density": [_vp, _vp, _l, _l, _vp, _l, _l, _vp, _vp],
+    "rkb_bspline_sym_matrix": [_vp, _i, _vp, _i, _i, _i, _vp, _vp, _l, _vp, _vp],
     "rkb_split_contract": [_vp, _vp, _l, _l, _i, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp,
                            _vp, _vp, _vp, _l, _vp, _vp, _vp],
 }

@@ -160,6 +160,26 @@ int rkb_table_contract_fp64_groups(const double *d_g, const double *d_y, long ld
                                    double *d_out, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Direct (Hartree) potential of the Dirac-Fock driver, the consumer of Y^0:
+ * atomx methods/dirac_fock.py:931-967 (DFSolver._build_direct_potential_yk)
+ * with numerics/bspline/integrals.py:18-56 (_assemble_integral).
+ *
+ * rkb_occupied_density: rho[i] = sum_o occ[o] (P[o][i]^2 + Q[o][i]^2), minus
+ * P[target][i]^2 + Q[target][i]^2 when target >= 0; orbital values are rows
+ * of leading dimension ld (n nodes); accumulated orbital by orbital in the
+ * reference's order.  d_occ is a device array of n_orb doubles.
+ *
+ * rkb_bspline_sym_matrix: the mm x mm matrix 0.5 (M + M^T) with
+ * M[gi][gj] = sum over cells iv of sum_m w[iv][m] f[iv][m] B1[iv][m][gi-iv]
+ * B2[iv][m][gj-iv] (0 <= gi-iv < ks1, 0 <= gj-iv < ks2; f may be NULL for 1),
+ * B1/B2 of shape (nv, ng, ks1/ks2); zero off the band.
+ * ------------------------------------------------------------------------- */
+int rkb_occupied_density(const double *d_P, const double *d_Q, long ld, long n_orb, const double *d_occ,
+                         long target, long n, double *d_rho, void *stream);
+int rkb_bspline_sym_matrix(const double *d_b1, int ks1, const double *d_b2, int ks2, int nv, int ng,
+                           const double *d_w, const double *d_f, long mm, double *d_out, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Split-precision engine (factored Green operator + CRT INT8 GEMMs).
  *
  * With g = w*rho, atomx's R^k(ac;bd) = g_ac^T G g_bd (numerics/yk.py:88 and

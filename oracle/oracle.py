@@ -17,6 +17,8 @@ its project root) in plain numpy or calls the C restatement in
 * ``coulomb_tables``        <- src/atomx/numerics/quadrature.py:190-231 (numpy)
 * ``yk_on_grid`` / ``grid_slater_rk`` / ``yk_pair_dot_batch_on_grid``
                             <- quadrature.py:234-404 (C, bit-faithful)
+* ``direct_potential_yk``   <- src/atomx/methods/dirac_fock.py:931-967 with
+                               numerics/bspline/integrals.py:18-56 (C)
 
 Parity of the oracle itself is pinned against vectors generated by running
 the reference (tests/golden/make_golden.py) and against closed forms.
@@ -313,3 +315,54 @@ def yk_pair_dot_batch_on_grid(PA, QA, PB, QB, rows_a, rows_b, rows_k, rows_ok, R
         _p(_c(inverse)), _p(_c(cuts, np.int64), _lptr), cuts.shape[0], _p(_c(transfers)), transfers.shape[1], ic,
         _p(val), threads)
     return val
+
+
+def _potential_lib():
+    lib = _lib()
+    if not getattr(lib, "_potential_ready", False):
+        lib.oracle_occupied_density.argtypes = [_dptr, _dptr, ctypes.c_long, ctypes.c_long, _dptr, ctypes.c_long,
+                                                ctypes.c_long, _dptr]
+        lib.oracle_occupied_density.restype = None
+        lib.oracle_bspline_sym_matrix.argtypes = [_dptr, ctypes.c_int, _dptr, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_int, _dptr, ctypes.c_long, _dptr]
+        lib.oracle_bspline_sym_matrix.restype = None
+        lib._potential_ready = True
+    return lib
+
+
+def direct_potential_yk(bsp_data, ns, orbitals, target_kappa=None, target_idx=None):
+    """(V_J_PP, V_J_QQ) <- src/atomx/methods/dirac_fock.py:931-967.
+
+    Orbital values as evaluate.py:71-97 (``eval_P``/``eval_Q``), the density
+    orbital by orbital in dict order (:939-952, C), Y^0 by ``yk_rows`` (C,
+    yk.py:88-154), weights grw * Y^0 (:955) and the symmetrised matrices of
+    ``_assemble_integral`` (numerics/bspline/integrals.py:18-56, C)."""
+    lib = _potential_lib()
+    nv, gr, grw = int(bsp_data["nv"]), np.asarray(bsp_data["gr"]), np.asarray(bsp_data["grw"])
+    ng = gr.shape[1]
+    n = nv * ng
+    Ps, Qs, occ, target = [], [], [], -1
+    for _kappa, orb_list in orbitals.items():
+        for P, Q, o in orb_list:
+            Ps.append(eval_P(P, bsp_data).ravel()), Qs.append(eval_Q(Q, bsp_data).ravel()), occ.append(float(o))
+    if target_kappa is not None and target_idx is not None:
+        lst = list(orbitals.get(target_kappa, []))
+        if target_idx < len(lst):
+            P, Q, _ = lst[target_idx]
+            Ps.append(eval_P(P, bsp_data).ravel()), Qs.append(eval_Q(Q, bsp_data).ravel()), occ.append(0.0)
+            target = len(Ps) - 1
+    rho = np.zeros(n)
+    if Ps:
+        Pm, Qm = np.ascontiguousarray(Ps), np.ascontiguousarray(Qs)
+        oc = np.ascontiguousarray(occ, dtype=np.float64)
+        lib.oracle_occupied_density(_p(Pm), _p(Qm), n, Pm.shape[0], _p(oc), target, n, _p(rho))
+    y = yk_rows(rho[None, :], 0, gr, grw, nv, ng)[0]
+    weights = np.ascontiguousarray(grw.ravel() * y)
+    out = []
+    for key, kkey in (("bsp_p", "ksp"), ("bsp_q", "ksq")):
+        b = np.ascontiguousarray(bsp_data[key], dtype=np.float64)
+        ks = int(bsp_data[kkey])
+        V = np.empty((int(ns), int(ns)))
+        lib.oracle_bspline_sym_matrix(_p(b), ks, _p(b), ks, nv, ng, _p(weights), int(ns), _p(V))
+        out.append(V)
+    return out[0], out[1]

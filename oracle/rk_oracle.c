@@ -306,3 +306,57 @@ void oracle_grid_pair_dot_batch(const double *PA, const double *QA, const double
                                  cons_rho, r, n, RK, inverse, cuts, ncuts, transfers, ntr, i_cut, val};
     parallel_for(grid_batch_range, &ctx, nrows, threads);
 }
+
+/* ------------------------------------------------------------------------
+ * Direct potential of the Dirac-Fock driver (atomx methods/dirac_fock.py:
+ * 931-967): the occupied density and the B-spline matrix of a weighted
+ * function (numerics/bspline/integrals.py:18-56 _assemble_integral).
+ * ---------------------------------------------------------------------- */
+
+/* rho[i] = sum_o occ[o] * (P[o][i]^2 + Q[o][i]^2), orbital by orbital as
+ * numpy's `rho_total += occ * (fP ** 2 + fQ ** 2)`; then minus the target's
+ * own P^2 + Q^2 (dirac_fock.py:939-952) when target >= 0. */
+void oracle_occupied_density(const double *P, const double *Q, long ld, long n_orb, const double *occ,
+                             long target, long n, double *rho)
+{
+    for (long i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (long o = 0; o < n_orb; ++o) {
+            const double p = P[o * ld + i], q = Q[o * ld + i];
+            acc += occ[o] * (p * p + q * q);
+        }
+        if (target >= 0) {
+            const double p = P[target * ld + i], q = Q[target * ld + i];
+            acc -= p * p + q * q;
+        }
+        rho[i] = acc;
+    }
+}
+
+/* mat (mm x mm, zeroed here) += the reference's cell loop: for each cell iv,
+ * basis pair (i, j) with gi = iv+i, gj = iv+j < mm, s = sum_m
+ * weights[iv][m] * b1[iv][m][i] * b2[iv][m][j]; then 0.5 * (mat + mat^T) as
+ * dirac_fock.py:960/965 does. */
+void oracle_bspline_sym_matrix(const double *b1, int ks1, const double *b2, int ks2, int nv, int ng,
+                               const double *weights, long mm, double *out)
+{
+    double *mat = calloc((size_t)(mm * mm), sizeof(double));
+    for (int iv = 0; iv < nv; ++iv)
+        for (int i = 0; i < ks1; ++i) {
+            const long gi = iv + i;
+            if (gi >= mm) continue;
+            for (int j = 0; j < ks2; ++j) {
+                const long gj = iv + j;
+                if (gj >= mm) continue;
+                double s = 0.0;
+                for (int m = 0; m < ng; ++m) {
+                    const long node = (long)iv * ng + m;
+                    s += weights[node] * b1[node * ks1 + i] * b2[node * ks2 + j];
+                }
+                mat[gi * mm + gj] += s;
+            }
+        }
+    for (long a = 0; a < mm; ++a)
+        for (long b = 0; b < mm; ++b) out[a * mm + b] = 0.5 * (mat[a * mm + b] + mat[b * mm + a]);
+    free(mat);
+}

@@ -26,6 +26,14 @@ atomx.  What each file holds:
 * hydrogenic.npz         atomx physics grid (ks=9, Z=1, r_max=50): nodes and
                          weights, atomx R^k for rho = 4 r^2 e^{-2r} (k=0..2)
                          and rho = e^{-r} (k=0..3) with 40-digit mpmath values.
+* direct_potential.npz   atomx DFSolver._build_direct_potential_yk
+                         (methods/dirac_fock.py:931-967) run unmodified on a
+                         stand-in ``self`` that carries only the attributes it
+                         reads (bsp_data, ns, ks and the two grid evaluators):
+                         the Z=10 ion with neon occupations and a 91-orbital
+                         batch ion with seeded fractional occupations, each
+                         with and without a target orbital.
+                         (``--only direct`` writes just this file.)
 * grid_quadrature.npz    atomx arbitrary-grid trapezoid Y^k (quadrature.py):
                          yk_on_grid / grid_slater_rk on a 1e-9..100 grid for
                          ranks up to 256, yk_pair_dot_batch_on_grid on the
@@ -109,10 +117,49 @@ def grid_quadrature():
     np.savez_compressed(os.path.join(HERE, "grid_quadrature.npz"), **out)
 
 
+def direct_potential():
+    """Inputs and outputs of atomx's direct-potential builder (see module doc)."""
+    from types import MethodType, SimpleNamespace
+
+    from atomx.methods.dirac_fock import DFSolver
+
+    from atomx_b200 import workloads as W
+
+    def run(ion, occ, target):
+        bd = ion.bsp
+        me = SimpleNamespace(bsp_data=bd, ns=int(bd["ns"]), ks=int(bd["ks"]))
+        me._eval_P_on_grid = MethodType(DFSolver._eval_P_on_grid, me)
+        me._eval_Q_on_grid = MethodType(DFSolver._eval_Q_on_grid, me)
+        orbitals = {}
+        for i, kappa in enumerate(ion.kappa):
+            orbitals.setdefault(int(kappa), []).append((ion.P[i], ion.Q[i], float(occ[i])))
+        plain = DFSolver._build_direct_potential_yk(me, orbitals)
+        tk, ti = target
+        minus = DFSolver._build_direct_potential_yk(me, orbitals, tk, ti)
+        return plain, minus
+
+    out = {}
+    cases = {"neon": (W.build_ion(W.neon_small()), None, (-1, 1)),
+             "batch5": (W.build_ion(W.uneven_batch()[5]), 7, (2, 3))}
+    for name, (ion, seed, target) in cases.items():
+        if seed is None:
+            occ = np.array([2.0, 2.0, 2.0, 4.0])  # 1s2 2s2 2p1/2^2 2p3/2^4
+        else:
+            occ = np.random.default_rng(seed).uniform(0.0, 2.0, size=ion.kappa.shape[0])
+        (vpp, vqq), (vpp_t, vqq_t) = run(ion, occ, target)
+        bd = ion.bsp
+        out.update({f"{name}_{k}": np.asarray(bd[k]) for k in ("gr", "grw", "bsp_p", "bsp_q")})
+        out.update({f"{name}_{k}": int(bd[k]) for k in ("nv", "ks", "ksp", "ksq", "nsp", "nsq", "ns")})
+        out.update({f"{name}_P": ion.P, f"{name}_Q": ion.Q, f"{name}_kappa": ion.kappa, f"{name}_occ": occ,
+                    f"{name}_target": np.array(target), f"{name}_VPP": vpp, f"{name}_VQQ": vqq,
+                    f"{name}_VPP_t": vpp_t, f"{name}_VQQ_t": vqq_t})
+    np.savez_compressed(os.path.join(HERE, "direct_potential.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--atomx-src", required=True)
-    ap.add_argument("--only", choices=["grid"], default=None,
+    ap.add_argument("--only", choices=["grid", "direct"], default=None,
                     help="write only one fixture family (the others are left as they are)")
     args = ap.parse_args()
     sys.path.insert(0, args.atomx_src)
@@ -120,6 +167,10 @@ def main():
     if args.only == "grid":
         grid_quadrature()
         print("golden grid fixtures written to", HERE)
+        return
+    if args.only == "direct":
+        direct_potential()
+        print("golden direct-potential fixtures written to", HERE)
         return
 
     from atomx.numerics.bspline.basis import prepare_bspline_data as ref_prepare
