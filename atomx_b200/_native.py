@@ -48,6 +48,7 @@ _SIGNATURES = {
     "rkb_split_certify": [_vp, _vp, _l, _vp, _vp, _d, _vp, _vp, _vp],
     "rkb_occupied_density": [_vp, _vp, _l, _l, _vp, _l, _l, _vp, _vp],
     "rkb_bspline_sym_matrix": [_vp, _i, _vp, _i, _i, _i, _vp, _vp, _l, _vp, _vp],
+    "rkb_exchange_matrix": [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp],
     "rkb_split_contract": [_vp, _vp, _l, _l, _i, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp,
                            _vp, _vp, _vp, _l, _vp, _vp, _vp],
 }

@@ -1,6 +1,7 @@
-// Direct (Hartree) potential matrices on the device: the consumer of the Y^k
-// kernel in atomx's Dirac-Fock driver (methods/dirac_fock.py:931-967,
-// DFSolver._build_direct_potential_yk).
+// One-electron potential matrices on the device built on Y^k: the direct
+// (Hartree) potential of atomx's Dirac-Fock driver (methods/dirac_fock.py:
+// 931-967, DFSolver._build_direct_potential_yk) and the non-local exchange
+// matrix of numerics/bspline/slater_yk.py:34-155 (below).
 //
 //   rho    = sum_o occ_o (P_o^2 + Q_o^2)  [- (P_t^2 + Q_t^2) for a target orbital]
 //   Y^0    = compute_yk(rho, k = 0)                      (rkb_yk_rows)
@@ -71,10 +72,89 @@ __global__ void sym_band_matrix_kernel(const double *__restrict__ b1, int ks1, c
     out[t] = __dmul_rn(0.5, __dadd_rn(a, b));
 }
 
+// ---------------------------------------------------------------------------
+// Exchange matrix K^k_{mn} = int B_m fb Y^k[fb B_n] with rectangle-rule
+// cumulative sums (atomx numerics/bspline/slater_yk.py:34-122,
+// _exchange_matrix_kernel).  One block per column n.  rho_n = fb B_n is
+// nonzero only on the cells [n-ks+1, n], so the outward sums are zero before
+// that support and a constant after it, and the inward sums the reverse:
+// thread 0 runs the two sequential sums over the support only, in the
+// reference's order, then every point gets
+//     Y^k_i = r_i^-(k+1) I_out(i) + r_i^k I_in(i)
+// and thread m accumulates K[m][n] cell by cell and node by node as the
+// reference does.  Shared memory: Y^k and w*fb for the whole row (2N doubles)
+// plus the support's two partial-sum arrays (2 * ks * ng doubles).
+__global__ void exchange_column_kernel(const double *__restrict__ fb, const double *__restrict__ bsp,
+                                       const double *__restrict__ r, const double *__restrict__ w, int nv, int ng,
+                                       int ks, int ns, int k, double *__restrict__ K) {
+    extern __shared__ double sx[];
+    const long N = (long)nv * ng;
+    double *yk = sx, *wfb = sx + N, *iout = wfb + N, *iin = iout + (long)ks * ng;
+    const int n_idx = blockIdx.x;
+    const int lo = n_idx - ks + 1 < 0 ? 0 : n_idx - ks + 1;
+    const int hi = n_idx + 1 > nv ? nv : n_idx + 1;  // cells [lo, hi)
+    const long p0 = (long)lo * ng, p1 = (long)hi * ng;  // support points [p0, p1)
+    for (long i = threadIdx.x; i < N; i += blockDim.x) wfb[i] = __dmul_rn(w[i], fb[i]);
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (long i = p0; i < p1; ++i) {
+            const int iv = (int)(i / ng), ls = n_idx - iv;
+            const double rho = __dmul_rn(fb[i], bsp[i * ks + ls]);
+            s = __dadd_rn(s, __dmul_rn(__dmul_rn(w[i], rho), int_pow(r[i], k)));
+            iout[i - p0] = s;
+        }
+        s = 0.0;
+        for (long i = p1 - 1; i >= p0; --i) {
+            const int iv = (int)(i / ng), ls = n_idx - iv;
+            const double rho = __dmul_rn(fb[i], bsp[i * ks + ls]);
+            s = __dadd_rn(s, __dmul_rn(__dmul_rn(w[i], rho), int_pow(r[i], -(k + 1))));
+            iin[i - p0] = s;
+        }
+    }
+    __syncthreads();
+    const double c_out = p1 > p0 ? iout[p1 - p0 - 1] : 0.0, c_in = p1 > p0 ? iin[0] : 0.0;
+    for (long i = threadIdx.x; i < N; i += blockDim.x) {
+        const double o = i < p0 ? 0.0 : (i < p1 ? iout[i - p0] : c_out);
+        const double in = i < p0 ? c_in : (i < p1 ? iin[i - p0] : 0.0);
+        yk[i] = __dadd_rn(__dmul_rn(int_pow(r[i], -(k + 1)), o), __dmul_rn(int_pow(r[i], k), in));
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < ns; m += blockDim.x) {
+        double kmn = 0.0;
+        const int c0 = m - ks + 1 < 0 ? 0 : m - ks + 1, c1 = m < nv - 1 ? m : nv - 1;
+        for (int iv = c0; iv <= c1; ++iv) {
+            const int sidx = m - iv;
+            double acc = 0.0;
+            for (int g = 0; g < ng; ++g) {
+                const long idx = (long)iv * ng + g;
+                acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(wfb[idx], bsp[idx * ks + sidx]), yk[idx]));
+            }
+            kmn = __dadd_rn(kmn, acc);
+        }
+        K[(long)m * ns + n_idx] = kmn;
+    }
+}
+
 }  // namespace potential
 }  // namespace rkb
 
 using namespace rkb;
+
+extern "C" int rkb_exchange_matrix(const double *d_fb, const double *d_bsp, const double *d_r, const double *d_w,
+                                   int nv, int ng, int ks, int ns, int k, double *d_K, void *stream) {
+    RKB_CHECK_ARG(nv >= 1 && ng >= 1 && ks >= 1 && ns >= 1 && ns <= nv + ks - 1, "invalid sizes");
+    RKB_CHECK_ARG(k >= 0, "multipole order must be >= 0 (got %d)", k);
+    RKB_CHECK_ARG(d_fb && d_bsp && d_r && d_w && d_K, "null argument");
+    const long n = (long)nv * ng;
+    const size_t smem = (size_t)(2 * n + 2L * ks * ng) * sizeof(double);
+    RKB_CHECK_ARG(smem <= 200 * 1024, "grid of %ld nodes too large for the exchange kernel", n);
+    RKB_CUDA(set_smem(potential::exchange_column_kernel, (int)smem));
+    const int threads = ns < 32 ? 32 : (ns > 1024 ? 1024 : (ns + 31) / 32 * 32);
+    potential::exchange_column_kernel<<<(unsigned)ns, threads, smem, as_stream(stream)>>>(d_fb, d_bsp, d_r, d_w, nv, ng,
+                                                                                         ks, ns, k, d_K);
+    RKB_LAUNCHED("exchange_column_kernel");
+    return RKB_OK;
+}
 
 extern "C" int rkb_occupied_density(const double *d_P, const double *d_Q, long ld, long n_orb, const double *d_occ,
                                     long target, long n, double *d_rho, void *stream) {

@@ -11,10 +11,17 @@ Mirrors atomx ``numerics/bspline/slater_yk.py``:
 
 The eight orbital evaluations run as two batched launches (P and Q
 components), followed by the pair densities, one Y^k row and one dot.
+
+* ``compute_exchange_matrix(orb_b_P, orb_b_Q, bsp_data, k)`` (:125) the
+  non-local exchange matrices K^k_PP (nsp x nsp, order-ksp basis) and K^k_QQ
+  (nsq x nsq, order-ksq basis) of ``_exchange_matrix_kernel`` (:34-122),
+  whose Y^k uses rectangle-rule cumulative sums: one ``rkb_exchange_matrix``
+  launch per block, one block per matrix column.
 """
 from __future__ import annotations
 
 import numpy as np
+import torch
 
 from . import _native
 from .device import as_device, resident
@@ -22,7 +29,7 @@ from .evaluate import eval_orbitals_on_grid
 from .slater import _dots
 from .yk import _check_k, _run_rows
 
-__all__ = ["compute_slater_rk", "compute_slater_fk", "compute_slater_gk"]
+__all__ = ["compute_slater_rk", "compute_slater_fk", "compute_slater_gk", "compute_exchange_matrix"]
 
 
 def compute_slater_rk(Pa, Qa, Pb, Qb, Pc, Qc, Pd, Qd, bsp_data, k):
@@ -62,3 +69,29 @@ def compute_slater_fk(orb_a_P, orb_a_Q, orb_b_P, orb_b_Q, bsp_data, k):
 def compute_slater_gk(orb_a_P, orb_a_Q, orb_b_P, orb_b_Q, bsp_data, k):
     """Exchange Slater integral G^k(a, b) = R^k(ab, ba)."""
     return compute_slater_rk(orb_a_P, orb_a_Q, orb_b_P, orb_b_Q, orb_b_P, orb_b_Q, orb_a_P, orb_a_Q, bsp_data, k)
+
+
+def compute_exchange_matrix(orb_b_P, orb_b_Q, bsp_data, k):
+    """(K_PP, K_QQ) as atomx compute_exchange_matrix (slater_yk.py:125-155)."""
+    if isinstance(k, bool) or int(k) != k or k < 0:
+        raise ValueError(f"k must be a non-negative integer (got {k!r})")
+    k = int(k)
+    L = _native.require_device()
+    nv = int(bsp_data["nv"])
+    ns = int(bsp_data["ns"])
+    gr, grw = bsp_data["gr"], bsp_data["grw"]
+    ng = gr.shape[1]
+    r, w = resident(np.asarray(gr).ravel()), resident(np.asarray(grw).ravel())
+    bsp_p = bsp_data["bsp_p"]
+    blocks = ((orb_b_P, bsp_p, int(bsp_data.get("ksp", bsp_data["ks"])), int(bsp_data.get("nsp", ns))),
+              (orb_b_Q, bsp_data.get("bsp_q", bsp_p), int(bsp_data.get("ksq", bsp_data["ks"])),
+               int(bsp_data.get("nsq", ns))))
+    out = []
+    for coeffs, bsp, ks, nsb in blocks:
+        fb = eval_orbitals_on_grid(as_device(np.asarray(coeffs, dtype=np.float64)), bsp, nv, ks, nsb)
+        b = resident(np.ascontiguousarray(bsp, dtype=np.float64))
+        K = torch.empty((nsb, nsb), dtype=torch.float64, device=fb.device)
+        _native.check(L.rkb_exchange_matrix(fb.data_ptr(), b.data_ptr(), r.data_ptr(), w.data_ptr(), nv, ng, ks, nsb,
+                                            k, K.data_ptr(), _native.stream_handle()), "rkb_exchange_matrix")
+        out.append(K.cpu().numpy())
+    return out[0], out[1]

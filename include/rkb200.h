@@ -179,6 +179,19 @@ int rkb_occupied_density(const double *d_P, const double *d_Q, long ld, long n_o
 int rkb_bspline_sym_matrix(const double *d_b1, int ks1, const double *d_b2, int ks2, int nv, int ng,
                            const double *d_w, const double *d_f, long mm, double *d_out, void *stream);
 
+/* rkb_exchange_matrix: the ns x ns non-local exchange matrix of atomx
+ * numerics/bspline/slater_yk.py:34-122 (_exchange_matrix_kernel, called by
+ * compute_exchange_matrix :125):
+ *     K[m][n] = sum_i w_i fb_i B_m(r_i) Y^k[fb B_n](r_i),
+ * Y^k from rectangle-rule cumulative sums (not the interpolatory rule of
+ * rkb_yk_rows): Y_i = r_i^-(k+1) sum_{j<=i} w_j rho_j r_j^k
+ *                   + r_i^k sum_{j>=i} w_j rho_j r_j^-(k+1).
+ * fb (nv*ng) is the orbital on the grid, bsp (nv, ng, ks) the B-spline
+ * values, r/w the flat grid, ns <= nv + ks - 1.  Every sum runs in the
+ * reference's order. */
+int rkb_exchange_matrix(const double *d_fb, const double *d_bsp, const double *d_r, const double *d_w, int nv,
+                        int ng, int ks, int ns, int k, double *d_K, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Split-precision engine (factored Green operator + CRT INT8 GEMMs).
  *

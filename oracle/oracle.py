@@ -19,6 +19,7 @@ its project root) in plain numpy or calls the C restatement in
                             <- quadrature.py:234-404 (C, bit-faithful)
 * ``direct_potential_yk``   <- src/atomx/methods/dirac_fock.py:931-967 with
                                numerics/bspline/integrals.py:18-56 (C)
+* ``compute_exchange_matrix`` <- src/atomx/numerics/bspline/slater_yk.py:34-155 (C)
 
 Parity of the oracle itself is pinned against vectors generated by running
 the reference (tests/golden/make_golden.py) and against closed forms.
@@ -365,4 +366,28 @@ def direct_potential_yk(bsp_data, ns, orbitals, target_kappa=None, target_idx=No
         V = np.empty((int(ns), int(ns)))
         lib.oracle_bspline_sym_matrix(_p(b), ks, _p(b), ks, nv, ng, _p(weights), int(ns), _p(V))
         out.append(V)
+    return out[0], out[1]
+
+
+def compute_exchange_matrix(orb_b_P, orb_b_Q, bsp_data, k):
+    """(K_PP, K_QQ) <- src/atomx/numerics/bspline/slater_yk.py:125-155 with the
+    kernel :34-122 (C): orbital values as evaluate.py:71-97."""
+    lib = _potential_lib()
+    if not getattr(lib, "_exchange_ready", False):
+        lib.oracle_exchange_matrix.argtypes = [_dptr, _dptr, _dptr, _dptr, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, _dptr]
+        lib.oracle_exchange_matrix.restype = None
+        lib._exchange_ready = True
+    nv, ns = int(bsp_data["nv"]), int(bsp_data["ns"])
+    gr = np.ascontiguousarray(np.asarray(bsp_data["gr"]).ravel())
+    grw = np.ascontiguousarray(np.asarray(bsp_data["grw"]).ravel())
+    ng = np.asarray(bsp_data["gr"]).shape[1]
+    out = []
+    for coeffs, key, kkey, nkey in ((orb_b_P, "bsp_p", "ksp", "nsp"), (orb_b_Q, "bsp_q", "ksq", "nsq")):
+        ks, nsb = int(bsp_data.get(kkey, bsp_data["ks"])), int(bsp_data.get(nkey, ns))
+        bsp = np.ascontiguousarray(bsp_data.get(key, bsp_data["bsp_p"]), dtype=np.float64)
+        fb = np.ascontiguousarray(eval_orbital_on_grid(coeffs, bsp, nv, ks, nsb).ravel())
+        K = np.empty((nsb, nsb))
+        lib.oracle_exchange_matrix(_p(fb), _p(bsp), _p(gr), _p(grw), nv, ng, ks, nsb, int(k), _p(K))
+        out.append(K)
     return out[0], out[1]

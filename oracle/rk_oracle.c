@@ -360,3 +360,57 @@ void oracle_bspline_sym_matrix(const double *b1, int ks1, const double *b2, int 
         for (long b = 0; b < mm; ++b) out[a * mm + b] = 0.5 * (mat[a * mm + b] + mat[b * mm + a]);
     free(mat);
 }
+
+/* Non-local exchange matrix K^k (atomx numerics/bspline/slater_yk.py:34-122,
+ * _exchange_matrix_kernel), restated loop by loop: r^k and r^-(k+1) by the
+ * integer power, integrand = (w fb) B_s, per column n the product density
+ * fb B_n on its cells, rectangle-rule outward/inward cumulative sums over
+ * the whole grid, Y^k = r^-(k+1) I_out + r^k I_in, then K[m][n] += sum_g
+ * integrand Y^k cell by cell.  fb (nv*ng), bsp (nv, ng, ks), K (ns x ns). */
+void oracle_exchange_matrix(const double *fb, const double *bsp, const double *gr, const double *grw, int nv,
+                            int ng, int ks, int ns, int k, double *K)
+{
+    const long n = (long)nv * ng;
+    double *rk = malloc(sizeof(double) * n), *rkm = malloc(sizeof(double) * n);
+    double *integ = malloc(sizeof(double) * n * ks), *rho = malloc(sizeof(double) * n);
+    double *iout = malloc(sizeof(double) * n), *iin = malloc(sizeof(double) * n), *yk = malloc(sizeof(double) * n);
+    memset(K, 0, sizeof(double) * (size_t)ns * ns);
+    for (long i = 0; i < n; ++i) {
+        rk[i] = oracle_int_pow(gr[i], k);
+        rkm[i] = oracle_int_pow(gr[i], -(long)(k + 1));
+    }
+    for (long i = 0; i < n; ++i) {
+        const double wfb = grw[i] * fb[i];
+        for (int s = 0; s < ks; ++s) integ[i * ks + s] = wfb * bsp[i * ks + s];
+    }
+    for (int nn = 0; nn < ns; ++nn) {
+        for (long i = 0; i < n; ++i) rho[i] = 0.0;
+        int lo = nn - ks + 1 < 0 ? 0 : nn - ks + 1, hi = nn + 1 > nv ? nv : nn + 1;
+        for (int iv = lo; iv < hi; ++iv)
+            for (int g = 0; g < ng; ++g) {
+                const long idx = (long)iv * ng + g;
+                rho[idx] = fb[idx] * bsp[idx * ks + (nn - iv)];
+            }
+        double s = 0.0;
+        for (long i = 0; i < n; ++i) {
+            s += grw[i] * rho[i] * rk[i];
+            iout[i] = s;
+        }
+        s = 0.0;
+        for (long i = n - 1; i >= 0; --i) {
+            s += grw[i] * rho[i] * rkm[i];
+            iin[i] = s;
+        }
+        for (long i = 0; i < n; ++i) yk[i] = rkm[i] * iout[i] + rk[i] * iin[i];
+        for (int iv = 0; iv < nv; ++iv)
+            for (int sidx = 0; sidx < ks; ++sidx) {
+                const int m = iv + sidx;
+                if (m < ns) {
+                    double acc = 0.0;
+                    for (int g = 0; g < ng; ++g) acc += integ[((long)iv * ng + g) * ks + sidx] * yk[(long)iv * ng + g];
+                    K[(long)m * ns + nn] += acc;
+                }
+            }
+    }
+    free(rk), free(rkm), free(integ), free(rho), free(iout), free(iin), free(yk);
+}

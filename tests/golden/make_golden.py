@@ -34,6 +34,10 @@ atomx.  What each file holds:
                          batch ion with seeded fractional occupations, each
                          with and without a target orbital.
                          (``--only direct`` writes just this file.)
+* exchange_matrix.npz    atomx compute_exchange_matrix (numerics/bspline/
+                         slater_yk.py:125, the rectangle-rule kernel :34-122)
+                         for orbitals of the Z=10 ion and of a batch ion at
+                         several k.  (``--only exchange`` writes just this file.)
 * grid_quadrature.npz    atomx arbitrary-grid trapezoid Y^k (quadrature.py):
                          yk_on_grid / grid_slater_rk on a 1e-9..100 grid for
                          ranks up to 256, yk_pair_dot_batch_on_grid on the
@@ -156,10 +160,30 @@ def direct_potential():
     np.savez_compressed(os.path.join(HERE, "direct_potential.npz"), **out)
 
 
+def exchange_matrix():
+    """Inputs and outputs of atomx compute_exchange_matrix (see module doc)."""
+    from atomx.numerics.bspline.slater_yk import compute_exchange_matrix
+
+    from atomx_b200 import workloads as W
+    out = {}
+    cases = {"neon": (W.build_ion(W.neon_small()), [(0, 0), (1, 1), (3, 2)]),
+             "batch5": (W.build_ion(W.uneven_batch()[5]), [(0, 0), (17, 3), (60, 6)])}
+    for name, (ion, picks) in cases.items():
+        bd = ion.bsp
+        out.update({f"{name}_{k}": np.asarray(bd[k]) for k in ("gr", "grw", "bsp_p", "bsp_q")})
+        out.update({f"{name}_{k}": int(bd[k]) for k in ("nv", "ks", "ksp", "ksq", "nsp", "nsq", "ns")})
+        out[f"{name}_picks"] = np.array(picks)
+        for orb, k in picks:
+            out[f"{name}_P{orb}"], out[f"{name}_Q{orb}"] = ion.P[orb], ion.Q[orb]
+            kpp, kqq = compute_exchange_matrix(ion.P[orb], ion.Q[orb], bd, k)
+            out[f"{name}_KPP_{orb}_{k}"], out[f"{name}_KQQ_{orb}_{k}"] = kpp, kqq
+    np.savez_compressed(os.path.join(HERE, "exchange_matrix.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--atomx-src", required=True)
-    ap.add_argument("--only", choices=["grid", "direct"], default=None,
+    ap.add_argument("--only", choices=["grid", "direct", "exchange"], default=None,
                     help="write only one fixture family (the others are left as they are)")
     args = ap.parse_args()
     sys.path.insert(0, args.atomx_src)
@@ -171,6 +195,10 @@ def main():
     if args.only == "direct":
         direct_potential()
         print("golden direct-potential fixtures written to", HERE)
+        return
+    if args.only == "exchange":
+        exchange_matrix()
+        print("golden exchange-matrix fixtures written to", HERE)
         return
 
     from atomx.numerics.bspline.basis import prepare_bspline_data as ref_prepare

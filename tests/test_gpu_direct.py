@@ -1,5 +1,7 @@
-"""Direct (Hartree) potential on the device (DFSolver._build_direct_potential_yk,
-atomx methods/dirac_fock.py:931-967) against atomx's outputs and the oracle.
+"""Potential matrices on the device against atomx's outputs and the oracle:
+the direct (Hartree) potential (DFSolver._build_direct_potential_yk, atomx
+methods/dirac_fock.py:931-967) and the exchange matrices
+(compute_exchange_matrix, numerics/bspline/slater_yk.py:125).
 
 The device evaluates the orbitals with its own reduction order, so the
 density and Y^0 differ from atomx's in the last bits; the matrices are
@@ -95,3 +97,59 @@ def test_errors():
     L = _native.load()
     with pytest.raises(ValueError):
         _native.check(L.rkb_occupied_density(0, 0, 10, 2, 0, 5, 10, 0, None), "rkb_occupied_density")
+
+
+# ------------------------------------------------------------------ exchange
+@pytest.fixture(scope="module")
+def gx():
+    return np.load(os.path.join(GOLDEN, "exchange_matrix.npz"))
+
+
+@pytest.mark.parametrize("name", ["neon", "batch5"])
+def test_exchange_matrix_matches_atomx(gx, name):
+    from test_oracle_exchange import exchange_case
+
+    from atomx_b200.slater_yk import compute_exchange_matrix
+    bd, picks = exchange_case(gx, name)
+    for orb, k in picks:
+        kpp, kqq = compute_exchange_matrix(gx[f"{name}_P{orb}"], gx[f"{name}_Q{orb}"], bd, k)
+        _close(kpp, gx[f"{name}_KPP_{orb}_{k}"])
+        _close(kqq, gx[f"{name}_KQQ_{orb}_{k}"])
+
+
+def test_exchange_kernel_equals_oracle_on_same_orbital(gx):
+    """Fed the oracle's own orbital values, the kernel runs every sum in the
+    reference's order: bit for bit."""
+    from test_oracle_exchange import exchange_case
+
+    from atomx_b200 import _native
+    L = _native.load()
+    bd, picks = exchange_case(gx, "batch5")
+    nv, ng = bd["gr"].shape
+    lib = oracle._potential_lib()
+    oracle.compute_exchange_matrix(gx["batch5_P0"], gx["batch5_Q0"], bd, 0)  # sets the C signatures
+    r = np.ascontiguousarray(bd["gr"].ravel())
+    w = np.ascontiguousarray(bd["grw"].ravel())
+    for orb, k in picks:
+        fb = np.ascontiguousarray(oracle.eval_P(gx[f"batch5_P{orb}"], bd).ravel())
+        b = np.ascontiguousarray(bd["bsp_p"])
+        ns = bd["nsp"]
+        ref = np.empty((ns, ns))
+        lib.oracle_exchange_matrix(oracle._p(fb), oracle._p(b), oracle._p(r), oracle._p(w), nv, ng, bd["ksp"], ns, k,
+                                   oracle._p(ref))
+        dfb, db, dr, dw = (torch.as_tensor(x, device="cuda") for x in (fb, b, r, w))
+        K = torch.empty((ns, ns), dtype=torch.float64, device="cuda")
+        _native.check(L.rkb_exchange_matrix(dfb.data_ptr(), db.data_ptr(), dr.data_ptr(), dw.data_ptr(), nv, ng,
+                                            bd["ksp"], ns, k, K.data_ptr(), None), "rkb_exchange_matrix")
+        np.testing.assert_array_equal(K.cpu().numpy(), ref)
+
+
+def test_exchange_errors(gx):
+    from test_oracle_exchange import exchange_case
+
+    from atomx_b200.slater_yk import compute_exchange_matrix
+    bd, _ = exchange_case(gx, "neon")
+    with pytest.raises(ValueError):
+        compute_exchange_matrix(gx["neon_P0"], gx["neon_Q0"], bd, -1)
+    with pytest.raises(ValueError):
+        compute_exchange_matrix(gx["neon_P0"], gx["neon_Q0"], bd, 1.5)
