@@ -60,8 +60,9 @@ def certify(grp_row0, grp_n, rowscale, cbound, limit: float, est, status, stream
 
 def read_status(status, stream):
     """Copy the device status words to pinned host memory on the stream the
-    work was enqueued on (None: the current stream) and wait for it: one
-    synchronisation.  Returns (stream, [words])."""
+    work was enqueued on (None: the current stream) and wait for that stream
+    (one synchronisation; the wait releases the GIL, unlike ``.item()``).
+    Returns (stream, [words])."""
     s = stream if stream is not None else torch.cuda.current_stream()
     host = torch.empty(status.shape, dtype=status.dtype, pin_memory=True)
     with torch.cuda.stream(s):
@@ -427,9 +428,10 @@ class SplitEngine:
         s = stream if stream is not None else torch.cuda.current_stream()
         plan = self.dev.plan
         self.rows(s)
-        # which tables go to FP64 is known from the rows alone: one wait here
-        with torch.cuda.stream(s):
-            flagged = int(self.status[1].item())
+        # which tables go to FP64 is known from the rows alone: one wait here,
+        # on this stream only and without holding the GIL (serving launches
+        # requests from several host threads)
+        _, (_, flagged) = read_status(self.status, s)
         fp64 = set(self._failing(self.est.cpu().numpy())) if flagged else set()
         self.escalated = sorted(fp64)
         nmax = max(plan.n_of_k(k) for k in plan.ks)
