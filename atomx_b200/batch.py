@@ -154,14 +154,39 @@ class SplitBatch(_Graphable):
     def ordered_entries(self) -> int:
         return sum(dv.plan.ordered_entries for dv in self.devs)
 
+    #: side streams the per-ion row launches are spread over
+    ROW_STREAMS = 4
+
     def rows(self, stream=None) -> None:
+        """Every ion's row kernels, then the certificate.  Ions on the cell or
+        fused kernel go round-robin to ROW_STREAMS side streams forked from and
+        joined back to ``stream`` (a fork/join that graph capture records), so
+        small ions fill the GPU side by side; two-kernel ions share the FP64
+        workspace and stay in order on ``stream``."""
+        s = stream if stream is not None else torch.cuda.current_stream()
         self._stream = stream
+        if not hasattr(self, "_side"):
+            self._side = [torch.cuda.Stream(device=s.device) for _ in range(self.ROW_STREAMS)]
+        fork = torch.cuda.Event()
+        fork.record(s)
+        used = set()
+        j = 0
         for i, r in enumerate(self.ions):
+            if r.kind == "two":
+                ls = s
+            else:
+                ls = self._side[j % len(self._side)]
+                j += 1
+                if ls not in used:
+                    ls.wait_event(fork)
+                    used.add(ls)
             r.launch(self.bits, self.n_mod, self._c[0], self.resA, self.resB, self.kpad, int(self.row_base[i]),
-                     self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp, self.xwork,
-                     stream)
-        certify(self.grp_row0, self.grp_n, self.rowscale, self.cbound, self.cert_limit, self.est, self.status,
-                stream)
+                     self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp, self.xwork, ls)
+        for ls in used:
+            join = torch.cuda.Event()
+            join.record(ls)
+            s.wait_event(join)
+        certify(self.grp_row0, self.grp_n, self.rowscale, self.cbound, self.cert_limit, self.est, self.status, s)
 
     def contract(self, stream=None) -> None:
         L = _native.load()

@@ -531,6 +531,8 @@ __global__ void __launch_bounds__(128) split_rows_fused_kernel(RowsArgs a) {
 //
 // Cell-minor factor table of one multipole (doubles), nv cells:
 //   u[NG][nv] | C[NG][nv] | L[NG][NG][nv] (L[i][node][m])
+constexpr int CELL_ZMAX = 128;  // Z columns per row of the cell kernel (one thread each, nv + Z <= 256)
+
 template <int NG>
 __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const double *__restrict__ ktab_t,
                                                               const long *__restrict__ koff_t) {
@@ -544,7 +546,7 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
     double *gimg = reinterpret_cast<double *>(smc);                  // [nv][GS]
     double *red = gimg + (size_t)nv * GS;                              // [64] block scratch
     unsigned char *lines = smc + ndbl * sizeof(double);               // [n_mod][kpad]
-    unsigned char *zneg = lines + (size_t)a.n_mod * kpad;             // [n_mod][64]: B's Z bytes
+    unsigned char *zneg = lines + (size_t)a.n_mod * kpad;             // [n_mod][CELL_ZMAX]: B's Z bytes
     const int k = a.row_k[q];
     const long pr = a.row_pair[q];
     const double *Pa = a.P + a.pairs[2 * pr] * a.orb_ld, *Pc = a.P + a.pairs[2 * pr + 1] * a.orb_ld;
@@ -698,7 +700,7 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
             lines[(size_t)md * kpad + kbody + e] = (unsigned char)r;
             int nr = -(int)(int8_t)(uint8_t)r;  // residue of -x, centred again
             nr -= nr > 127 ? a.mod[md] : 0;
-            zneg[md * 64 + e] = (unsigned char)nr;
+            zneg[md * CELL_ZMAX + e] = (unsigned char)nr;
         }
     }
     __syncthreads();
@@ -718,7 +720,7 @@ __global__ void __launch_bounds__(256) split_rows_cell_kernel(RowsArgs a, const 
                 *reinterpret_cast<uint4 *>(tmp) = v;
                 for (int b = 0; b < 16; ++b) {
                     const long c = ch * 16 + b;
-                    if (c >= kbody && c < zend) tmp[b] = zneg[md * 64 + (c - kbody)];
+                    if (c >= kbody && c < zend) tmp[b] = zneg[md * CELL_ZMAX + (c - kbody)];
                 }
                 *reinterpret_cast<uint4 *>(a.resB + o) = *reinterpret_cast<const uint4 *>(tmp);
             } else {
@@ -1249,7 +1251,8 @@ extern "C" int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long
                                     long kpad, long row_base, long nrows_total, double *d_rowscale, double *d_left,
                                     double *d_right, double *d_cbound, int cwp, void *stream) {
     RKB_CHECK_ARG(nv >= 2 && ng >= 5 && ng <= 11, "the cell row kernel takes 5 <= ng <= 11 (got %d)", ng);
-    RKB_CHECK_ARG(max_z >= 0 && max_z <= 64, "the cell row kernel takes <= 64 Z columns (got %d)", max_z);
+    RKB_CHECK_ARG(max_z >= 0 && max_z <= CELL_ZMAX, "the cell row kernel takes <= %d Z columns (got %d)", CELL_ZMAX,
+                  max_z);
     const long threads = ((long)nv + max_z + 31) / 32 * 32;
     RKB_CHECK_ARG(threads <= 256, "grid too long for the cell row kernel (%d cells + %d Z columns > 256)", nv,
                   max_z);
@@ -1276,7 +1279,7 @@ extern "C" int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long
     a.resA = d_resA; a.resB = d_resB; a.kpad = kpad; a.row_base = row_base; a.nrows_total = nrows_total;
     a.rowscale = d_rowscale; a.left = d_left; a.right = d_right; a.cbound = d_cbound; a.cwp = cwp;
     RKB_CHECK_ARG(d_ktab_t != nullptr && d_koff_t != nullptr, "the cell-minor factor tables are required");
-    const size_t smem = ((((size_t)nv * (ng | 1) + 64 + 1) & ~(size_t)1) * sizeof(double)) + (size_t)n_mod * (kpad + 64);
+    const size_t smem = ((((size_t)nv * (ng | 1) + 64 + 1) & ~(size_t)1) * sizeof(double)) + (size_t)n_mod * (kpad + CELL_ZMAX);
     RKB_CHECK_ARG(smem <= 200 * 1024, "row images too large for shared memory");
     cudaStream_t st = as_stream(stream);
     const dim3 grid((unsigned)nrows), block((unsigned)threads);

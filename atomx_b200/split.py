@@ -159,6 +159,7 @@ def host_tables(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
     return out
 
 
+CELLS_Z_MAX = 128  # Z columns per row of the cell-parallel row kernel
 FUSED_PASSES_MAX = 32  # passes of 32 // ng cells kept in registers by the fused row kernel
 FUSED_Z_MAX = 64
 
@@ -171,7 +172,7 @@ def fused_fits(nv: int, ng: int, max_z: int) -> bool:
 def cells_fit(nv: int, ng: int, max_z: int) -> bool:
     """Whether the cell-parallel row kernel takes this grid (one block of at
     most 256 threads: a thread per cell plus one per Z column)."""
-    return 5 <= ng <= 11 and max_z <= 64 and -(-(nv + max_z) // 32) * 32 <= 256
+    return 5 <= ng <= 11 and max_z <= CELLS_Z_MAX and -(-(nv + max_z) // 32) * 32 <= 256
 
 
 def fused_body_width(nv: int, ng: int) -> int:

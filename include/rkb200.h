@@ -262,7 +262,7 @@ int rkb_split_rows_fused(const double *d_Pv, const double *d_Qv, long orb_ld, co
 
 /* rkb_split_rows_cells: the rkb_split_rows computation with one block per
  * row and one thread per cell (5 <= ng <= 11, nv + max_z <= 256 threads,
- * max_z <= 64), no FP64 workspace; residue columns in natural order
+ * max_z <= 128), no FP64 workspace; residue columns in natural order
  * ((m-1)*ng + node, then Z), positions from (nv-1)*ng + nZ up to kpad
  * written as zeros.  Besides the packed tables (d_ktab/d_koff) it reads a
  * cell-minor copy of each multipole's factors at d_ktab_t + d_koff_t[k]:

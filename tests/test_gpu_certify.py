@@ -84,6 +84,44 @@ def test_row_record_and_certificate_match_emulation(cancelling, rows_kernel):
     assert flagged == int(np.sum(~(est <= eng.cert_limit))) >= 1
 
 
+def test_cell_kernel_with_more_than_64_z_columns():
+    """Ion 43 (nv 98, ng 9, up to 65 Z columns) runs on the cell kernel: its
+    residues rebuild [X | Z] to the rounding quantum and B negates Z."""
+    from atomx_b200.split import SplitEngine
+    from split_emulation import crt_exact
+    ion, Pg, Qg, dev = _ion(43)
+    eng = SplitEngine(dev)
+    assert eng.ion_rows.kind == "cells" and eng.max_z > 64
+    eng.rows()
+    torch.cuda.synchronize()
+    plan = dev.plan
+    nv, ng = ion.bsp["gr"].shape
+    resA = eng.resA.cpu().numpy().astype(np.int64)
+    resB = eng.resB.cpu().numpy().astype(np.int64)
+    rs = eng.rowscale.cpu().numpy()
+    flat, koff = eng.ktab.cpu().numpy(), eng.koff.cpu().numpy()
+    rng = np.random.default_rng(43)
+    for k in plan.ks:
+        if eng.nz[k] <= 64:
+            continue
+        F = unpack_table(flat, int(koff[k]), nv, ng)
+        off, nk = plan.k_row_offset[k], plan.n_of_k(k)
+        rows = np.sort(rng.choice(nk, size=min(12, nk), replace=False)) + off
+        rho = np.array([Pg[a] * Pg[c] + Qg[a] * Qg[c] for a, c in plan.pairs[plan.row_pair[rows]]])
+        X, Z, _, _ = transform_rows(rho * ion.bsp["grw"].reshape(1, -1), F, nv, ng)
+        ref = np.concatenate([X, Z], axis=1)
+        pos = eng.column_positions(k)
+        got = crt_exact([resA[i][rows][:, pos] for i in range(eng.n_mod)], eng.moduli) * rs[rows][:, None]
+        assert np.all(np.abs(got - ref) <= (0.5 + 1e-6) * rs[rows][:, None] + 1e-15 * np.abs(ref)), k
+        zpos = pos[X.shape[1]:]
+        xb = crt_exact([resB[i][rows][:, zpos] for i in range(eng.n_mod)], eng.moduli)
+        xa = crt_exact([resA[i][rows][:, zpos] for i in range(eng.n_mod)], eng.moduli)
+        np.testing.assert_array_equal(xb, -xa)
+        break
+    else:
+        pytest.fail("no multipole with more than 64 Z columns")
+
+
 def test_single_ion_recomputes_failing_tables_in_fp64(cancelling):
     from atomx_b200.split import SplitEngine
     from atomx_b200.tables import tables_for

@@ -38,6 +38,7 @@ def test_split_width_choice():
 def test_row_kernel_fit_rules():
     from atomx_b200.split import cells_fit, fused_body_positions, fused_body_width, fused_fits
     assert cells_fit(112, 8, 37) and cells_fit(192, 11, 64) and not cells_fit(200, 11, 64)
+    assert cells_fit(98, 9, 65) and cells_fit(120, 9, 128) and not cells_fit(100, 9, 129)
     assert not cells_fit(100, 4, 0) and not cells_fit(100, 12, 0)
     assert fused_fits(112, 8, 37) and not fused_fits(192, 11, 10)
     for nv, ng in [(112, 8), (34, 7), (60, 5), (30, 11)]:
