@@ -18,6 +18,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+import threading
+
 import numpy as np
 
 from .angular import exchange_k_range
@@ -66,8 +68,33 @@ class TablePlan:
         return [(int(bid[a]), int(a), int(b)) for a, b in zip(starts, stops)]
 
 
+_plan_cache: dict = {}
+_plan_lock = threading.Lock()
+
+
 def make_plan(kappa, k_max: int) -> TablePlan:
+    """The table plan of an orbital set (see TablePlan); cached by the kappa
+    sequence and k_max, since it depends on nothing else.  Plans are shared:
+    treat their arrays as read-only."""
     kappa = np.asarray(kappa, dtype=np.int64)
+    key = (kappa.tobytes(), int(k_max)) if kappa.ndim == 1 else None
+    if key is not None:
+        with _plan_lock:
+            hit = _plan_cache.get(key)
+        if hit is not None:
+            return hit
+    plan = _make_plan(kappa, k_max)
+    if key is not None:
+        for a in (plan.kappa, plan.pairs, plan.pair_block, plan.row_pair, plan.row_k, *plan.pairs_of_k.values()):
+            a.setflags(write=False)
+        with _plan_lock:
+            if len(_plan_cache) > 1024:
+                _plan_cache.clear()
+            plan = _plan_cache.setdefault(key, plan)
+    return plan
+
+
+def _make_plan(kappa, k_max: int) -> TablePlan:
     n = kappa.shape[0]
     if n == 0:
         raise ValueError("an ion needs at least one spinor")
@@ -76,31 +103,35 @@ def make_plan(kappa, k_max: int) -> TablePlan:
     # Shells: maximal runs of equal kappa in orbital order.
     starts = [0] + [i for i in range(1, n) if kappa[i] != kappa[i - 1]]
     shells = [(int(kappa[s]), s, (starts[j + 1] if j + 1 < len(starts) else n)) for j, s in enumerate(starts)]
-    pairs, pblock, blocks = [], [], []
-    allowed_of_block = []
+    pair_parts, block_parts, blocks, allowed_of_block = [], [], [], []
+    count = 0
     for i, (ka, sa, ea) in enumerate(shells):
         for j in range(i, len(shells)):
             kc, sc, ec = shells[j]
-            start = len(pairs)
-            for a in range(sa, ea):
-                c0 = a if i == j else sc
-                for c in range(c0, ec):
-                    pairs.append((a, c))
-            blocks.append((ka, kc, start, len(pairs)))
+            if i == j:  # a <= c within the shell, a-major order
+                a, c = np.triu_indices(ea - sa)
+                a, c = a + sa, c + sa
+            else:
+                a = np.repeat(np.arange(sa, ea), ec - sc)
+                c = np.tile(np.arange(sc, ec), ea - sa)
+            pair_parts.append(np.stack([a, c], axis=1))
+            block_parts.append(np.full(a.shape[0], len(blocks), dtype=np.int64))
+            blocks.append((ka, kc, count, count + a.shape[0]))
+            count += a.shape[0]
             allowed_of_block.append([k for k in exchange_k_range(ka, kc) if k <= k_max])
-            pblock += [len(blocks) - 1] * (len(pairs) - start)
-    pairs = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
-    pblock = np.asarray(pblock, dtype=np.int64)
+    pairs = np.concatenate(pair_parts).astype(np.int64).reshape(-1, 2)
+    pblock = np.concatenate(block_parts)
     ks = sorted({k for al in allowed_of_block for k in al})
     pairs_of_k = {}
     for k in ks:
         idx = [np.arange(b[2], b[3]) for bi, b in enumerate(blocks) if k in allowed_of_block[bi]]
         pairs_of_k[k] = np.concatenate(idx).astype(np.int64) if idx else np.zeros(0, np.int64)
-    row_pair, row_k, off = [], [], {}
+    off, pos = {}, 0
     for k in ks:
-        off[k] = len(row_pair)
-        row_pair.extend(pairs_of_k[k].tolist())
-        row_k.extend([k] * pairs_of_k[k].shape[0])
+        off[k] = pos
+        pos += pairs_of_k[k].shape[0]
+    row_pair = np.concatenate([pairs_of_k[k] for k in ks]) if ks else np.zeros(0, np.int64)
+    row_k = np.concatenate([np.full(pairs_of_k[k].shape[0], k, dtype=np.int64) for k in ks]) if ks else \
+        np.zeros(0, np.int64)
     return TablePlan(kappa=kappa, pairs=pairs, pair_block=pblock, blocks=blocks, ks=ks,
-                     pairs_of_k=pairs_of_k, row_pair=np.asarray(row_pair, dtype=np.int64),
-                     row_k=np.asarray(row_k, dtype=np.int64), k_row_offset=off)
+                     pairs_of_k=pairs_of_k, row_pair=row_pair.astype(np.int64), row_k=row_k, k_row_offset=off)

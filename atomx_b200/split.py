@@ -160,6 +160,21 @@ def host_tables(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
 
 
 CELLS_Z_MAX = 128  # Z columns per row of the cell-parallel row kernel
+def _device_table(H: dict, key: str, device) -> torch.Tensor:
+    """Device copy of one of a cached host-table set's arrays, kept with the set
+    (the set is immutable and cached by grid content, so the copy is reused by
+    every engine on that grid and device)."""
+    cache = H.setdefault("_device", {})
+    ck = (key, str(device))
+    with _factor_lock:
+        t = cache.get(ck)
+    if t is None:
+        t = torch.as_tensor(H[key], device=device)
+        with _factor_lock:
+            t = cache.setdefault(ck, t)
+    return t
+
+
 FUSED_PASSES_MAX = 32  # passes of 32 // ng cells kept in registers by the fused row kernel
 FUSED_Z_MAX = 64
 
@@ -218,8 +233,8 @@ class IonRows:
         self.factors = H["factors"]
         kmax = max(plan.ks)
         d = dev.Pv.device
-        self.ktab = torch.as_tensor(H["flat"], device=d)
-        self.koff = torch.as_tensor(H["koff"], device=d)
+        self.ktab = _device_table(H, "flat", d)
+        self.koff = _device_table(H, "koff", d)
         self.kbody = (nv - 1) * ng
         self.nz = dict(H["nz"])
         max_z = max(self.nz.values())
@@ -255,8 +270,8 @@ class IonRows:
         self.fused = kind == "fused"
         self.ktab_t = self.koff_t = None
         if kind == "cells":  # cell-minor copy of u, ell, C and L for coalesced per-cell reads
-            self.ktab_t = torch.as_tensor(H["flat_t"], device=d)
-            self.koff_t = torch.as_tensor(H["koff_t"], device=d)
+            self.ktab_t = _device_table(H, "flat_t", d)
+            self.koff_t = _device_table(H, "koff_t", d)
         self.max_z = max_z
         self.body_w = fused_body_width(nv, ng) if self.fused else self.kbody
         self.kdim = {k: _round_up(self.body_w + self.nz[k], self.KCHUNK) for k in plan.ks}
@@ -452,6 +467,42 @@ class SplitEngine:
         self._streamed = True
         if check:
             self.check_status()
+
+    def run_to_host(self, host: torch.Tensor, stream=None, copy_stream=None) -> None:
+        """The whole table into ``host`` (pinned, ``total`` doubles): the rows
+        and the certificate, then each multipole's table is contracted (or
+        recomputed in FP64 when its certificate failed) on ``stream`` and copied
+        to the host on ``copy_stream`` while the next one is contracted.
+        Returns once the host copy is complete; raises like check_status()."""
+        if self.out is None:
+            raise ValueError("this engine streams its tables (materialize=False); use stream_tables()")
+        if host.numel() < self.total or host.is_cuda:
+            raise ValueError(f"host buffer must be a CPU tensor of at least {self.total} doubles")
+        s = stream if stream is not None else torch.cuda.current_stream()
+        cs = copy_stream if copy_stream is not None else self.__dict__.setdefault(
+            "_copy_stream", torch.cuda.Stream(device=self.out.device))
+        plan = self.dev.plan
+        self.rows(s)
+        _, (_, flagged) = read_status(self.status, s)  # which tables go to FP64: one wait
+        fp64 = set(self._failing(self.est.cpu().numpy())) if flagged else set()
+        self.escalated = sorted(fp64)
+        for gi, k in enumerate(plan.ks):
+            nk, o = plan.n_of_k(k), self.offsets[k]
+            if k in fp64:
+                self._recompute(((k, o),)).run(self.out, s)
+            else:
+                t0, t1 = self.task_range[gi]
+                self._contract(self.grp_out, t0, t1, self.out, s)
+            ev = torch.cuda.Event()
+            ev.record(s)
+            cs.wait_event(ev)
+            with torch.cuda.stream(cs):
+                host[o:o + nk * nk].copy_(self.out[o:o + nk * nk], non_blocking=True)
+        self._streamed = True  # the per-table route is already taken
+        try:
+            self.check_status()
+        finally:
+            cs.synchronize()
 
     def run(self, stream=None, upload: bool = True, check: bool = True) -> torch.Tensor:
         self.rows(stream)

@@ -29,7 +29,7 @@ from .yk import yk_partial_matrices
 
 __all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "upload_ion", "upload_values", "slater_rk_tables",
            "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE",
-           "Fp64Recompute"]
+           "Fp64Recompute", "fp64_tables_to_host"]
 
 TILE = 128
 
@@ -80,12 +80,26 @@ def upload_ion(ion, k_max: int | None = None, plan: TablePlan | None = None, str
                                       bsp["nsp"], Pv.data_ptr(), n, s), "rkb_eval_orbitals(P)")
     _native.check(L.rkb_eval_orbitals(cq.data_ptr(), cq.shape[1], n_orb, bq.data_ptr(), nv, ng, bsp["ksq"],
                                       bsp["nsq"], Qv.data_ptr(), n, s), "rkb_eval_orbitals(Q)")
-    dev = cp.device
+    pairs, row_pair, row_k = _plan_arrays(plan)
     return IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=r, w=w, mo=mo, mi=mi, Pv=Pv, Qv=Qv,
-                     pairs=torch.as_tensor(plan.pairs.reshape(-1), device=dev),
-                     row_pair=torch.as_tensor(plan.row_pair, device=dev),
-                     row_k=torch.as_tensor(plan.row_k.astype(np.int32), device=dev),
+                     pairs=pairs, row_pair=row_pair, row_k=row_k,
                      extra={"r_host": np.asarray(bsp["gr"], dtype=np.float64).reshape(-1)})
+
+
+def _plan_arrays(plan: TablePlan):
+    """Device copies of a plan's pair and row arrays, kept with the (cached,
+    read-only) plan object per device."""
+    key = str(torch.device("cuda", torch.cuda.current_device()))
+    cache = plan.__dict__.setdefault("_device", {})
+    hit = cache.get(key)
+    if hit is None:
+        dev = torch.device(key)
+        # (the plan's arrays are read-only; torch wants writable sources)
+        hit = (torch.from_numpy(plan.pairs.reshape(-1).copy()).to(dev),
+               torch.from_numpy(plan.row_pair.copy()).to(dev),
+               torch.from_numpy(plan.row_k.astype(np.int32)).to(dev))
+        hit = cache.setdefault(key, hit)
+    return hit
 
 
 def upload_values(Pv, Qv, kappa, gr, grw, k_max: int, plan: TablePlan | None = None) -> IonDevice:
@@ -100,12 +114,10 @@ def upload_values(Pv, Qv, kappa, gr, grw, k_max: int, plan: TablePlan | None = N
     mo_h, mi_h = yk_partial_matrices(ng)
     Pd = as_device(Pv).reshape(-1, n).contiguous()
     Qd = as_device(Qv).reshape(-1, n).contiguous()
-    dev = Pd.device
+    pairs, row_pair, row_k = _plan_arrays(plan)
     return IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=resident(gr).reshape(-1), w=resident(grw).reshape(-1),
                      mo=resident(mo_h), mi=resident(mi_h), Pv=Pd, Qv=Qd,
-                     pairs=torch.as_tensor(plan.pairs.reshape(-1), device=dev),
-                     row_pair=torch.as_tensor(plan.row_pair, device=dev),
-                     row_k=torch.as_tensor(plan.row_k.astype(np.int32), device=dev),
+                     pairs=pairs, row_pair=row_pair, row_k=row_k,
                      extra={"r_host": None if isinstance(gr, torch.Tensor) else np.asarray(gr, dtype=np.float64).reshape(-1)})
 
 
@@ -238,8 +250,36 @@ class Fp64Recompute:
                                                        out.data_ptr(), s), "rkb_table_contract_fp64_groups")
 
 
+def fp64_tables_to_host(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, host: torch.Tensor, stream=None,
+                        copy_stream=None) -> None:
+    """Plain FP64 engine with each multipole's table copied to ``host`` on
+    ``copy_stream`` while the next one is contracted; returns when done."""
+    L = _native.load()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    cs = copy_stream if copy_stream is not None else torch.cuda.Stream(device=out.device)
+    h = _native.stream_handle(s)
+    plan = dev.plan
+    _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                        dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                        dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
+                                        dev.mi.data_ptr(), ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, h),
+                  "rkb_table_rows_fp64")
+    for gi, k in enumerate(plan.ks):
+        t0, t1 = ws.task_range[gi]
+        nk, o = plan.n_of_k(k), ws.offsets[k]
+        _native.check(L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
+                                                ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr() + 12 * t0,
+                                                t1 - t0, out.data_ptr(), h), "rkb_table_contract_fp64")
+        ev = torch.cuda.Event()
+        ev.record(s)
+        cs.wait_event(ev)
+        with torch.cuda.stream(cs):
+            host[o:o + nk * nk].copy_(out[o:o + nk * nk], non_blocking=True)
+    cs.synchronize()
+
+
 def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, sink=None,
-                     **split_opts):
+                     host: bool = False, **split_opts):
     """All R^k tables of one ion on the device (see module docstring).
 
     With ``sink`` the tables are streamed instead of returned: the engine
@@ -250,13 +290,17 @@ def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", str
     before returning).  ``iter_blocks`` splits it into (k, kappa_ac-block,
     kappa_bd-block) tiles; ``HostTableSink`` copies tables to pinned host
     memory.  Returns an ``RkStream`` summary in that case.
+
+    With ``host=True`` the tables come back in pinned host memory
+    (``values`` is a CPU tensor): each multipole's table is copied while the
+    next one is contracted, so the device-to-host copy hides the compute.
     """
     if precision not in ("fp64", "split"):
         raise ValueError(f"unknown precision {precision!r}; choose 'fp64' or 'split'")
     dev = upload_ion(ion, k_max=k_max, stream=stream)
     if sink is not None:
         return stream_tables(dev, sink, precision=precision, stream=stream, **split_opts)
-    return tables_for(dev, precision=precision, stream=stream, **split_opts)
+    return tables_for(dev, precision=precision, stream=stream, host=host, **split_opts)
 
 
 @dataclass
@@ -344,14 +388,24 @@ def slater_rk_tables_from_values(Pv, Qv, kappa, gr, grw, k_max: int, precision: 
     return tables_for(dev, precision=precision, stream=stream, **split_opts)
 
 
-def tables_for(dev: IonDevice, precision: str = "fp64", stream=None, **split_opts) -> RkTables:
+def tables_for(dev: IonDevice, precision: str = "fp64", stream=None, host: bool = False,
+               **split_opts) -> RkTables:
     if precision == "split":
         from .split import SplitEngine
         eng = SplitEngine(dev, **split_opts)
-        out = eng.run(stream=stream, check=True)
-        return RkTables(plan=dev.plan, ks=dev.plan.ks, values=out, offsets=eng.offsets, precision="split",
+        if host:
+            values = torch.empty(eng.total, dtype=torch.float64, pin_memory=True)
+            eng.run_to_host(values, stream=stream)
+        else:
+            values = eng.run(stream=stream, check=True)
+        return RkTables(plan=dev.plan, ks=dev.plan.ks, values=values, offsets=eng.offsets, precision="split",
                         info=eng.info())
     ws = Fp64Workspace(dev)
     out = torch.empty(ws.total, device=dev.Pv.device, dtype=torch.float64)
-    run_fp64(dev, ws, out, stream=stream)
-    return RkTables(plan=dev.plan, ks=dev.plan.ks, values=out, offsets=ws.offsets, precision="fp64")
+    if host:
+        values = torch.empty(ws.total, dtype=torch.float64, pin_memory=True)
+        fp64_tables_to_host(dev, ws, out, values, stream=stream)
+    else:
+        run_fp64(dev, ws, out, stream=stream)
+        values = out
+    return RkTables(plan=dev.plan, ks=dev.plan.ks, values=values, offsets=ws.offsets, precision="fp64")
