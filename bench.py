@@ -391,6 +391,8 @@ def run_gpu(args):
         line["grid_yk"] = grid_leg()
     if not args.no_batch and engine == "split":
         line["batch"] = batch_leg()
+    if not args.no_stream and engine == "split":
+        line["stream"] = stream_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
@@ -553,6 +555,47 @@ def grid_leg(rows: int = 4000, n: int = 20000, reps: int = 5) -> dict:
             "algorithmic_gbs": bytes_row * rows / (ms / 1e3) / 1e9}
 
 
+def stream_leg(reps: int = 2) -> dict:
+    """The Z=54 CI table (N=2112 with 11 Gauss nodes per cell, 300 spinors,
+    k <= 16: 1.95e9 ordered entries, 15.6 GB as FP64) streamed multipole by
+    multipole to a device sink that reduces every table (per-row sums), split
+    and FP64 in turn; the engine never holds the whole table.  CUDA events
+    around each whole stream on the launching stream."""
+    import torch
+
+    from atomx_b200 import tables as T
+    from atomx_b200 import workloads as W
+    from atomx_b200.serve import ChecksumSink
+    spec = W.xenon_ci_table()
+    dev = T.upload_ion(W.build_ion(spec))
+    entries = dev.plan.ordered_entries
+    s = torch.cuda.current_stream()
+    out = {"workload": "xenon_ci_table: Z=54, 200 B-splines order 9, n_gauss=11 (N=2112), 300 spinors "
+                       "kappa+-1..+-9, k<=16", "entries": entries, "table_bytes": entries * 8,
+           "sink": "device: per-row sums of every multipole table"}
+    for precision in ("split", "fp64"):
+        ts, held, info = [], 0, {}
+        for i in range(reps + 1):
+            sink = ChecksumSink()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            summary = T.stream_tables(dev, sink, precision=precision, stream=s)
+            e1.record(s)
+            torch.cuda.synchronize()
+            if i:
+                ts.append(e0.elapsed_time(e1))
+            held, info = summary.device_bytes, summary.info
+        ms = statistics.median(ts)
+        out[precision] = {"ms": ms, "integrals_per_s": entries / (ms / 1e3), "engine_device_bytes": held}
+        if precision == "split":
+            out[precision]["fp64_multipoles"] = info.get("fp64_multipoles")
+            out[precision]["bits"], out[precision]["rows_kernel"] = info.get("bits"), info.get("rows_kernel")
+        torch.cuda.empty_cache()
+    out["speedup_split_vs_fp64"] = out["fp64"]["ms"] / out["split"]["ms"]
+    return out
+
+
 def batch_leg(reps: int = 3) -> dict:
     """The 64-ion uneven batch (Z 20..83, 40..160 B-splines of order 7 or 9,
     20..150 spinors, k_max = 12): every table of every ion in one persistent
@@ -627,6 +670,7 @@ def main():
     ap.add_argument("--serve", type=int, default=32, help="requests in the serving leg (0 = skip)")
     ap.add_argument("--no-grid", action="store_true", help="skip the arbitrary-grid Y^k leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-ion batch leg")
+    ap.add_argument("--no-stream", action="store_true", help="skip the streamed Z=54 CI table leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
