@@ -385,13 +385,17 @@ def run_gpu(args):
             "roofline": dom, "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "clocks": clk.summary(), "wall_s": t_wall}
     line.update(extra)
-    if args.serve > 0 and engine == "split":
+    # the other workloads (serving, arbitrary grids, the 64-ion batch, the
+    # streamed CI table) are measured once, on one GPU: under torchrun every
+    # rank would only repeat them while all N GPUs are held
+    extra_legs = engine == "split" and world == 1
+    if args.serve > 0 and extra_legs:
         line["serve"] = serve_leg(args)
-    if not args.no_grid and engine == "split":
+    if not args.no_grid and extra_legs:
         line["grid_yk"] = grid_leg()
-    if not args.no_batch and engine == "split":
+    if not args.no_batch and extra_legs:
         line["batch"] = batch_leg()
-    if not args.no_stream and engine == "split":
+    if not args.no_stream and extra_legs:
         line["stream"] = stream_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ion, plan)
