@@ -417,10 +417,23 @@ class SplitEngine:
         certify(self.grp_row0, self.grp_n, self.rowscale, self.cbound, self.cert_limit, self.est, self.status,
                 stream)
 
+    #: when a list, contract() appends a (start, end) CUDA event pair around
+    #: each contraction launch, recorded on the launch stream (live timing of
+    #: the dominant kernel inside a caller's timed region)
+    kernel_events = None
+
     def contract(self, stream=None) -> None:
         if self.out is None:
             raise ValueError("this engine streams its tables (materialize=False); use stream_tables()")
-        self._contract(self.grp_out, 0, self.n_tasks, self.out, stream)
+        if self.kernel_events is None:
+            self._contract(self.grp_out, 0, self.n_tasks, self.out, stream)
+            return
+        s = stream if stream is not None else torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        self._contract(self.grp_out, 0, self.n_tasks, self.out, s)
+        b.record(s)
+        self.kernel_events.append((a, b))
 
     def _contract(self, grp_out, t0, t1, out, stream) -> None:
         L = _native.load()
@@ -553,22 +566,28 @@ class SplitEngine:
                 "device_bytes": self.device_bytes(),
                 "tasks": self.n_tasks}
 
-    def roofline(self, stream=None, flush=None, reps: int = 3) -> dict:
-        """Dominant kernel (K3s) alone, timed with CUDA events on ``stream``."""
+    def roofline(self, stream=None, flush=None, reps: int = 3, kernel_ms: float | None = None) -> dict:
+        """Roofline of the dominant kernel (K3s): its duration ``kernel_ms``
+        (e.g. the mean of the launches recorded through ``kernel_events``
+        inside a timed region), or else timed alone with CUDA events on
+        ``stream`` over ``reps`` launches."""
         import json
         import os
-        s = stream or torch.cuda.current_stream()
-        self.rows(s)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-        for a, b in ev:
-            if flush is not None:
-                flush.zero_()
-            a.record(s)
-            self.contract(s)
-            b.record(s)
-        torch.cuda.synchronize()
-        self.check_status()
-        ms = float(np.median([a.elapsed_time(b) for a, b in ev]))
+        if kernel_ms is None:
+            s = stream or torch.cuda.current_stream()
+            self.rows(s)
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+            for a, b in ev:
+                if flush is not None:
+                    flush.zero_()
+                a.record(s)
+                self.contract(s)
+                b.record(s)
+            torch.cuda.synchronize()
+            self.check_status()
+            ms = float(np.median([a.elapsed_time(b) for a, b in ev]))
+        else:
+            ms = float(kernel_ms)
         plan = self.dev.plan
         # algorithmic work: 2 * kdim int8 ops per modulus for every unique
         # entry (i <= j) of every table; the tiles actually issued also cover
