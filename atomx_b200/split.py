@@ -451,9 +451,12 @@ class SplitEngine:
     def stream_tables(self, sink, stream=None, check: bool = True) -> None:
         """Compute the rows once, then each multipole's table into one of two
         rotating device buffers and hand it to ``sink(k, table, blocks, stream)``
-        (see ``tables.stream_tables``); the whole table is never held.  With
-        ``check=False`` nothing waits for the device (call ``check_status()``
-        once the stream's work is known to be done)."""
+        (see ``tables.stream_tables``); the whole table is never held.  The
+        call waits once, after the row kernels, for the per-table certificate
+        (tables that fail it are recomputed in FP64 before they reach the
+        sink).  With ``check=False`` nothing else waits for the device: call
+        ``check_status()`` once the stream's work is known to be done, to
+        raise a contraction error."""
         s = stream if stream is not None else torch.cuda.current_stream()
         plan = self.dev.plan
         self.rows(s)
