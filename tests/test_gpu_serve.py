@@ -6,7 +6,6 @@ requests in flight, and then each request alone. Every table of every request
 must be identical in both runs, since no request's work depends on another's.
 The report carries p50/p99 latency and throughput.
 """
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu

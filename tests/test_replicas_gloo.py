@@ -9,7 +9,6 @@ sharding of the uneven batch.
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 from conftest import ROOT

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from split_emulation import crt_value, residues, transform_rows, unpack_table
+from split_emulation import crt_value, transform_rows, unpack_table
 
 
 def _ion_rows(name, n_pairs=120, seed=0):
