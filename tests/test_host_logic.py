@@ -80,3 +80,26 @@ def test_serving_footprint_grows_with_the_request():
     assert 0 < fs < fb and ff > 0
     # the split estimate covers the residue matrices of that ion (11 moduli, two copies)
     assert fb > 2 * 11 * 56209 * 1024
+
+
+def test_plan_is_cached_read_only_and_ordered():
+    from atomx_b200 import plan as PL
+    from atomx_b200 import workloads as W
+    kappa = W.build_ion(W.ytterbium_scaleup()).kappa
+    p = PL.make_plan(kappa, 12)
+    assert PL.make_plan(np.array(kappa), 12) is p and PL.make_plan(kappa, 11) is not p
+    for a in (p.pairs, p.row_pair, p.row_k, p.pair_block):
+        assert not a.flags.writeable
+    # pairs: block by block, a-major; a <= c inside a shell block
+    for bi, (ka, kc, s0, s1) in enumerate(p.blocks):
+        blk = p.pairs[s0:s1]
+        assert np.all(p.pair_block[s0:s1] == bi) and np.all(kappa[blk[:, 0]] == ka) and np.all(kappa[blk[:, 1]] == kc)
+        order = blk[:, 0] * len(kappa) + blk[:, 1]
+        assert np.all(np.diff(order) > 0)
+        if ka == kc:
+            assert np.all(blk[:, 0] <= blk[:, 1])
+    # rows: grouped by k in increasing order, each group the pairs of that k
+    for k in p.ks:
+        o, n = p.k_row_offset[k], p.n_of_k(k)
+        assert np.array_equal(p.row_pair[o:o + n], p.pairs_of_k[k]) and np.all(p.row_k[o:o + n] == k)
+    assert p.row_pair.shape[0] == sum(p.n_of_k(k) for k in p.ks) == p.n_rows
