@@ -71,3 +71,33 @@ def test_realtime_stream_reports_latency_and_admits_by_memory():
     assert rep2.max_inflight_seen == 1 and all(r.error is None for r in reqs2)
     server.close()
     small.close()
+
+
+def test_served_cancelling_ion_is_within_the_gate():
+    """A request whose k=7 table fails the split certificate (ion 42 of the
+    uneven batch) served in a mix: its streamed tables take the FP64 route
+    and every table is within 1e-10 (Schwarz-relative) of the FP64 engine."""
+    from atomx_b200 import workloads as W
+    from atomx_b200.serve import Request, SlaterServer
+    from atomx_b200.tables import tables_for, upload_ion
+    spec = W.uneven_batch()[42]
+    ion = W.build_ion(spec)
+    target = Request(rid=99, ion=ion, k_max=spec.k_max, sink=_Collect())
+    others = [r for r, _ in _requests(n=4, seed=4203)]
+    for r in others:
+        r.sink = _Collect()
+    server = SlaterServer(precision="split", max_inflight=4)
+    server.serve([target] + others, realtime=False)
+    torch.cuda.synchronize()
+    assert target.error is None and all(r.error is None for r in others)
+    plain = tables_for(upload_ion(ion, k_max=spec.k_max), "fp64")
+    assert sorted(target.sink.tables) == sorted(plain.ks)
+    worst = 0.0
+    for k, t in target.sink.tables.items():
+        ref = plain.table(k)
+        d = torch.diagonal(ref).abs().sqrt()
+        worst = max(worst, float(((t - ref).abs() / torch.outer(d, d)).max()))
+    assert worst <= 1e-10, worst
+    # the cancelling table itself came from the FP64 engine
+    assert float((target.sink.tables[7] - plain.table(7)).abs().max()) <= 1e-14 * float(plain.table(7).abs().max())
+    server.close()
