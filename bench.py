@@ -270,6 +270,7 @@ def table_errors(test, ref, offsets, plan):
     """
     import torch
     schwarz = floored = absmax = 0.0
+    per_k = {}
     for k in plan.ks:
         nk = plan.n_of_k(k)
         o = offsets[k]
@@ -278,12 +279,14 @@ def table_errors(test, ref, offsets, plan):
         d = (t - r).abs()
         dg = r.diagonal().abs().sqrt()
         scale = torch.outer(dg, dg)
-        schwarz = max(schwarz, float((d / scale).max()))
+        ks_ = float((d / scale).max())
         floor = 1e-6 * float(r.abs().max())
-        floored = max(floored, float((d / r.abs().clamp_min(floor)).max()))
-        absmax = max(absmax, float(d.max()))
+        kf = float((d / r.abs().clamp_min(floor)).max())
+        ka = float(d.max())
+        per_k[str(k)] = {"schwarz_rel": ks_, "rel_floored_1e-6": kf, "abs": ka}
+        schwarz, floored, absmax = max(schwarz, ks_), max(floored, kf), max(absmax, ka)
         del d, scale
-    return {"max_schwarz_rel": schwarz, "max_rel_floored_1e-6": floored, "max_abs": absmax}
+    return {"max_schwarz_rel": schwarz, "max_rel_floored_1e-6": floored, "max_abs": absmax, "per_table": per_k}
 
 
 def profiled_traffic(kernel: str, plan):
