@@ -34,12 +34,34 @@ _lock = threading.Lock()
 _cache: dict = {}
 
 
+def _frame_starts(r, k_max):
+    """First index of every frame, plus len(r) at the end.
+
+    Each frame holds the points whose radius lies within a factor
+    e^(128/(k_max+1)) of the frame's first radius.  Within such a frame
+    (r/r0)^k and (r/r0)^-(k+1) stay inside e^(+-128) for every k <= k_max,
+    far inside the double range, whatever the grid spans overall.  A frame
+    always takes at least one point, so the walk ends.
+    """
+    log_r = np.log(r)
+    width = 128.0 / (k_max + 1)
+    starts = [0]
+    while starts[-1] < r.shape[0]:
+        first = starts[-1]
+        beyond = int(np.searchsorted(log_r, log_r[first] + width, side="right"))
+        starts.append(beyond if beyond > first else first + 1)
+    return np.asarray(starts, dtype=np.int64)
+
+
 def coulomb_tables(r, k_max):
     """(rk, inverse, cuts, transfers) of a grid, as numpy arrays.
 
-    Frames start at cuts[b]; within frame b, x = r / r[cuts[b]] spans at most
-    e^(128 / (k_max + 1)), rk[k] = x^k and inverse[k] = x^-(k+1) / r[cuts[b]];
-    transfers[k][b] = (r[cuts[b]] / r[cuts[b+1]])^k.
+    ``cuts`` are the frame starts (``_frame_starts``).  With r0 the first
+    radius of a point's frame and x = r / r0: rk[k] = x^k and
+    inverse[k] = x^-(k+1) / r0.  A moment carried from one frame to the next
+    is multiplied by transfers[k][b] = (r0_b / r0_{b+1})^k, which is <= 1
+    because the grid increases, so carries only shrink when they change
+    frame.
     """
     if isinstance(k_max, (bool, np.bool_)) or int(k_max) != k_max or k_max < 0:
         raise ValueError('Coulomb multipole rank must be a nonnegative integer')
@@ -48,23 +70,21 @@ def coulomb_tables(r, k_max):
     if (r.ndim != 1 or not r.size or not np.isfinite(r).all()
             or np.any(r <= 0) or np.any(np.diff(r) <= 0)):
         raise ValueError('Coulomb grid must be finite, positive and strictly increasing')
-    logs, cuts = np.log(r), [0]
-    span = 128. / (k_max + 1)
-    while cuts[-1] < len(r):
-        stop = int(np.searchsorted(logs, logs[cuts[-1]] + span, side='right'))
-        cuts.append(max(cuts[-1] + 1, stop))
-    cuts = np.asarray(cuts, dtype=np.int64)
-    anchors = r[cuts[:-1]]
-    orders = np.arange(k_max + 1)[:, None]
-    rk = np.empty((k_max + 1, len(r)))
+    starts = _frame_starts(r, k_max)
+    ranks = np.arange(k_max + 1)[:, None]  # integer exponents, as numpy's ** takes them
+    rk = np.empty((k_max + 1, r.shape[0]))
     inverse = np.empty_like(rk)
-    for b in range(len(anchors)):
-        lo, hi = cuts[b:b + 2]
-        x = r[lo:hi] / anchors[b]
-        rk[:, lo:hi] = x[None, :] ** orders
-        inverse[:, lo:hi] = x[None, :] ** (-orders - 1) / anchors[b]
-    transfers = (anchors[:-1] / anchors[1:])[None, :] ** np.arange(k_max + 1)[:, None]
-    return rk, inverse, cuts, transfers
+    for lo, hi in zip(starts[:-1].tolist(), starts[1:].tolist()):
+        r0 = r[lo]
+        x = r[lo:hi] / r0
+        # fresh results from integer exponents: numpy's vectorised pow and
+        # its scalar pow can differ in the last bit, and which one runs
+        # depends on the operands' types and strides
+        rk[:, lo:hi] = x[None, :] ** ranks
+        inverse[:, lo:hi] = x[None, :] ** (-1 - ranks) / r0
+    first = r[starts[:-1]]
+    transfers = (first[:-1] / first[1:])[None, :] ** ranks
+    return rk, inverse, starts, transfers
 
 
 class GridTables:

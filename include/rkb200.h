@@ -327,8 +327,10 @@ int rkb_split_certify(const long *d_grp_row0, const long *d_grp_n, long n_groups
  * (16 MiB of doubles, held on every GPU that loads the library until exit);
  * larger requests return RKB_EINVAL.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) with that device current;
- * make it before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race, so serialise them.
+ * make it before any stream capture.  The address is kept for the life of the
+ * process, so the library must not be used across a cudaDeviceReset of that
+ * device.  All calls share the array: calls that overlap on the GPU race, so
+ * serialise them.
  * ------------------------------------------------------------------------- */
 #define RKB_SPLIT_ROWS_NOALLOC_MAX_DOUBLES (2L * 1024L * 1024L)
 

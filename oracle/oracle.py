@@ -59,6 +59,9 @@ def _lib():
     lib.oracle_dot_table.argtypes = [_dptr, _dptr, ctypes.c_long, _lptr, _lptr, ctypes.c_long,
                                      _dptr, ctypes.c_int]
     lib.oracle_dot_table.restype = None
+    lib.oracle_dot_block.argtypes = [_dptr, ctypes.c_long, _dptr, ctypes.c_long, ctypes.c_long, _dptr,
+                                     ctypes.c_int]
+    lib.oracle_dot_block.restype = None
     lib.oracle_int_pow.argtypes = [ctypes.c_double, ctypes.c_long]
     lib.oracle_int_pow.restype = ctypes.c_double
     lib.oracle_max_threads.restype = ctypes.c_int
@@ -126,6 +129,19 @@ def dot_entries(g: np.ndarray, y: np.ndarray, ia, ib, threads: int = 0) -> np.nd
     out = np.empty(ia.shape[0])
     _lib().oracle_dot_table(_p(g), _p(y), g.shape[1], _p(ia, _lptr), _p(ib, _lptr), ia.shape[0],
                             _p(out), int(threads))
+    return out
+
+
+def dot_block(g: np.ndarray, y: np.ndarray, threads: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+    """out[j, i] = g[i] . y[j]: every row of g against every row of y, one
+    plain dot per entry (the per-integral sum of slater_rk_poisson)."""
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    assert g.shape[1] == y.shape[1]
+    if out is None:
+        out = np.empty((y.shape[0], g.shape[0]))
+    assert out.shape == (y.shape[0], g.shape[0]) and out.flags.c_contiguous and out.dtype == np.float64
+    _lib().oracle_dot_block(_p(g), g.shape[0], _p(y), y.shape[0], g.shape[1], _p(out), int(threads))
     return out
 
 

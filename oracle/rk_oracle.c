@@ -18,7 +18,7 @@
  *   oracle_dot_table  <- src/atomx/numerics/bspline/slater.py:118-130
  *       (slater_rk_poisson: R = sum_i w_i rho13_i Y[rho24]_i), one plain
  *       dot per ordered table entry, as the reference evaluates it per
- *       integral.
+ *       integral; oracle_dot_block is the same dot over a block of a table.
  *
  *   oracle_grid_*     <- src/atomx/numerics/quadrature.py:247-391 (trapezoid Y^k
  *       on arbitrary grids; see the section at the end of this file).
@@ -168,6 +168,33 @@ void oracle_dot_table(const double *g, const double *y, long n,
 {
     struct dot_ctx c = {g, y, ia, ib, out, n};
     parallel_for(dot_range, &c, nent, threads);
+}
+
+/* out[j*na + i] = sum_x g[i][x] * y[j][x] for every i < na, j < nb: the
+ * per-entry dot of oracle_dot_table over a block of a table (every row a of a
+ * multipole group against the Y^k rows b listed in y), without index arrays.
+ * One plain dot per ordered entry, as slater.py:130 evaluates each integral. */
+struct block_ctx { const double *g, *y; double *out; long n, na; };
+
+static void block_range(void *vctx, long lo, long hi)
+{
+    struct block_ctx *c = (struct block_ctx *)vctx;
+    for (long j = lo; j < hi; ++j) {
+        const double *b = c->y + j * c->n;
+        double *o = c->out + j * c->na;
+        for (long i = 0; i < c->na; ++i) {
+            const double *a = c->g + i * c->n;
+            double s = 0.0;
+            for (long x = 0; x < c->n; ++x) s += a[x] * b[x];
+            o[i] = s;
+        }
+    }
+}
+
+void oracle_dot_block(const double *g, long na, const double *y, long nb, long n, double *out, int threads)
+{
+    struct block_ctx c = {g, y, out, n, na};
+    parallel_for(block_range, &c, nb, threads);
 }
 
 /* ------------------------------------------------------------------------

@@ -23,7 +23,28 @@ def test_reference_arm_prints_one_contract_line():
     assert line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
-    assert line["config"]["entries_per_step"] == 318112753
+    # one step is slice 0 of 4: every 4th bd row of each multipole table
+    # against all of its ac rows, measured (nothing extrapolated)
+    from atomx_b200 import plan as PL
+    from atomx_b200 import workloads as W
+    spec = W.ytterbium_scaleup()
+    plan = PL.make_plan(W.build_ion(spec).kappa, spec.k_max)
+    assert plan.ordered_entries == 318112753
+    want = sum(((plan.n_of_k(k) + 3) // 4) * plan.n_of_k(k) for k in plan.ks)
+    assert line["config"]["entries_per_step"] == want
+    assert abs(line["ms_per_step"] - line["cpu_baseline"]["seconds_measured"] * 1e3) < 20.0
+
+
+def test_reference_slices_cover_the_table_once():
+    import numpy as np
+
+    from atomx_b200 import plan as PL
+    from bench import REFERENCE_SLICES
+    plan = PL.make_plan(np.array([-1, -1, 1, -2, -2, 2, -3]), 4)
+    for k in plan.ks:
+        nk = plan.n_of_k(k)
+        seen = np.concatenate([np.arange(p, nk, REFERENCE_SLICES) for p in range(REFERENCE_SLICES)])
+        assert np.array_equal(np.sort(seen), np.arange(nk))
 
 
 def test_reference_arm_other_ranks_exit_without_work():

@@ -5,7 +5,9 @@ Tolerances:
 * Y^k rows: |Y - Y_ref| <= 1e-13 max|Y_ref| per row (the device scan only
   re-associates the cross-cell base sums; measured ~1e-16).
 * R^k entries: Schwarz-relative error |R - R_ref| / sqrt(|R_acac R_bdbd|)
-  <= 1e-13, and plain relative <= 1e-12 where |R_ref| >= 1e-3 of that scale.
+  <= 1e-13, and plain relative <= 1e-12 where |R_ref| >= 1e-3 of that scale
+  and <= 1e-13 where |R_ref| >= 5e-2 of it (the floored-relative metric over
+  the most cancelling entries is in test_gpu_accuracy.py).
 """
 import os
 
@@ -217,9 +219,12 @@ def _schwarz_check(tab, k, oracle_vals, idx_i, idx_j, gate=1e-13):
     scale = np.sqrt(diag[idx_i] * diag[idx_j])
     err = np.abs(got - oracle_vals) / scale
     assert err.max() <= gate, (k, err.max())
-    big = np.abs(oracle_vals) >= 1e-3 * scale
-    rel = np.abs(got - oracle_vals)[big] / np.abs(oracle_vals[big])
-    assert rel.size == 0 or rel.max() <= 1e-12, (k, rel.max())
+    # plain relative error: an FP64 error of ~1e-15 of the Schwarz scale is
+    # 1e-12 of an entry at 1e-3 of its scale, 2e-14 at 5e-2
+    for frac, rel_gate in ((1e-3, 1e-12), (5e-2, 1e-13)):
+        big = np.abs(oracle_vals) >= frac * scale
+        rel = np.abs(got - oracle_vals)[big] / np.abs(oracle_vals[big])
+        assert rel.size == 0 or rel.max() <= rel_gate, (k, frac, rel.max())
 
 
 def test_fp64_table_neon_every_entry(neon):
@@ -276,3 +281,36 @@ def test_fp64_table_from_coefficients_ytterbium():
         A, B = a.table(k), b.table(k)
         d = torch.sqrt(torch.outer(torch.diagonal(B).abs(), torch.diagonal(B).abs()))
         assert float(((A - B).abs() / d).max()) <= 1e-10, k
+
+
+def test_pair_density_entry_point_matches_oracle_bitwise(neon):
+    """rkb_pair_density (atomx slater_yk.py:193-194, rho = P_aP_c + Q_aQ_c)
+    through the C ABI: every pair of the Z=10 table, with strided rows,
+    equal to the oracle bit for bit (two products, one add, no fused
+    multiply-add on either side)."""
+    from atomx_b200 import _native
+    L = _native.require_device()
+    g, _ = neon
+    Pg, Qg, pairs = g["Pg"], g["Qg"], np.ascontiguousarray(g["pairs"], dtype=np.int64)
+    n_orb, n = Pg.shape
+    ld = n + 5
+    P = torch.zeros((n_orb, ld), dtype=torch.float64, device="cuda")
+    Q = torch.zeros_like(P)
+    P[:, :n] = torch.from_numpy(Pg)
+    Q[:, :n] = torch.from_numpy(Qg)
+    dp = torch.from_numpy(pairs).cuda()
+    rho_ld = n + 3
+    rho = torch.full((pairs.shape[0], rho_ld), -7.0, dtype=torch.float64, device="cuda")
+    _native.check(L.rkb_pair_density(P.data_ptr(), Q.data_ptr(), ld, dp.data_ptr(), pairs.shape[0], n,
+                                     rho.data_ptr(), rho_ld, None), "rkb_pair_density")
+    torch.cuda.synchronize()
+    got = rho.cpu().numpy()
+    ref = np.array([oracle.pair_density(Pg[a], Qg[a], Pg[c], Qg[c]) for a, c in pairs])
+    assert np.array_equal(got[:, :n], ref)
+    assert np.all(got[:, n:] == -7.0)  # padding columns untouched
+    # an empty pair list is a no-op; a leading dimension below n is refused
+    _native.check(L.rkb_pair_density(P.data_ptr(), Q.data_ptr(), ld, dp.data_ptr(), 0, n, rho.data_ptr(),
+                                     rho_ld, None))
+    with pytest.raises(ValueError):
+        _native.check(L.rkb_pair_density(P.data_ptr(), Q.data_ptr(), n - 1, dp.data_ptr(), 1, n, rho.data_ptr(),
+                                         rho_ld, None))

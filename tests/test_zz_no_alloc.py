@@ -32,25 +32,35 @@ def _outputs(torch, eng, nr):
                 cbound=torch.empty((nr, CB_STRIDE), dtype=torch.float64, device=d))
 
 
-def _call(torch, eng, r0, nr, noalloc):
-    """Rows [r0, r0 + nr) of eng's plan into fresh output buffers."""
+def _call(torch, eng, r0, nr, noalloc, row_base=0):
+    """Rows [r0, r0 + nr) of eng's plan into fresh output buffers.
+
+    The rows land at output rows [row_base, row_base + nr); the entry points
+    index their workspace the same way, so a caller workspace of
+    (row_base + nr) rows is what rkb_split_rows needs.  Only the written rows
+    are returned.
+    """
     from atomx_b200 import _native
     L = _native.load()
     dev = eng.dev
-    out = _outputs(torch, eng, nr)
+    total = row_base + nr
+    out = _outputs(torch, eng, total)
     head = (dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
             dev.row_pair.data_ptr() + 8 * r0, dev.row_k.data_ptr() + 4 * r0, nr, dev.w.data_ptr(), dev.nv,
             dev.ng, eng.ktab.data_ptr(), eng.koff.data_ptr(), eng.bits, eng.n_mod, eng._mod_c[0],
-            out["resA"].data_ptr(), _native.ptr(out["resB"]), eng.kpad, 0, nr, out["rowscale"].data_ptr(),
-            out["left"].data_ptr(), out["right"].data_ptr(), out["cbound"].data_ptr(), eng.cwp)
+            out["resA"].data_ptr(), _native.ptr(out["resB"]), eng.kpad, row_base, total,
+            out["rowscale"].data_ptr(), out["left"].data_ptr(), out["right"].data_ptr(),
+            out["cbound"].data_ptr(), eng.cwp)
     if noalloc:
         st = L.rkb_split_rows_noalloc(*head, eng.zcount.data_ptr(), None)
     else:
-        xwork = torch.empty((nr, eng.kpad), dtype=torch.float64, device=eng.ktab.device)
+        xwork = torch.empty((total, eng.kpad), dtype=torch.float64, device=eng.ktab.device)
         st = L.rkb_split_rows(*head, xwork.data_ptr(), eng.zcount.data_ptr(), None)
     _native.check(st, "rkb_split_rows_noalloc" if noalloc else "rkb_split_rows")
     torch.cuda.synchronize()
-    return out
+    sl = slice(row_base, total)
+    return {key: (None if v is None else (v[:, sl] if key in ("resA", "resB") else v[sl]))
+            for key, v in out.items()}
 
 
 def _same(a, b):
@@ -94,6 +104,20 @@ def test_noalloc_rows_match_caller_workspace_twice():
     got3 = _call(torch, neon, 0, n1, noalloc=True)
     _same(ref1, got3)
 
-    # a request beyond the fixed workspace is refused before any launch
+    # rows placed at an offset: row_base + nrows is exactly the capacity, so
+    # the last row ends on the last double of the fixed workspace
+    base = 700
+    nb = CAP // yb.kpad - base
+    ref4 = _call(torch, yb, 1234, nb, noalloc=False, row_base=base)
+    got4 = _call(torch, yb, 1234, nb, noalloc=True, row_base=base)
+    _same(ref4, got4)
+    assert bool((got4["resA"] != 0).any())
+
+    # a request beyond the fixed workspace is refused before any launch,
+    # whether the rows alone or the offset plus the rows overflow it
     with pytest.raises(ValueError, match="fixed workspace"):
         _call(torch, yb, 0, nr + 1, noalloc=True)
+    with pytest.raises(ValueError, match="fixed workspace"):
+        _call(torch, yb, 0, nb + 1, noalloc=True, row_base=base)
+    with pytest.raises(ValueError, match="fixed workspace"):
+        _call(torch, yb, 0, 1, noalloc=True, row_base=CAP // yb.kpad)
