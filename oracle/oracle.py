@@ -49,8 +49,9 @@ def build() -> str:
 
 @lru_cache(maxsize=1)
 def _lib():
-    if not os.path.exists(_LIB_PATH) or (
-            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "rk_oracle.c"))):
+    if not os.path.exists(_LIB_PATH) or any(
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, src))
+            for src in ("rk_oracle.c", "cell_oracle.c")):
         build()
     lib = ctypes.CDLL(_LIB_PATH)
     lib.oracle_yk_rows.argtypes = [_dptr, _iptr, ctypes.c_long, _dptr, _dptr, ctypes.c_int,

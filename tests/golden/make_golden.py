@@ -44,6 +44,11 @@ atomx.  What each file holds:
                          reference's batch geometry and on a make_fine_grid
                          grid with seeded waves, and the endpoint cases.
                          (``--only grid`` writes just this file.)
+* convol.npz             atomx's cell (bank) engine, numerics/bspline/convol.py:
+                         whole banks on a tiny basis, cell Slater integrals
+                         (scalar and batched), bilinear tables, direct and
+                         exchange matrices and DBSR Fock blocks (see
+                         ``convol_fixtures``).  (``--only convol``.)
 """
 from __future__ import annotations
 
@@ -180,10 +185,159 @@ def exchange_matrix():
     np.savez_compressed(os.path.join(HERE, "exchange_matrix.npz"), **out)
 
 
+def convol_fixtures():
+    """Golden vectors of atomx's cell (bank) R^k engine, numerics/bspline/convol.py.
+
+    * tiny: a 14-spline order-5 kinetically balanced basis on which whole
+      banks fit a fixture: ConvolCache.get_rkb for all four component types at
+      k = 0, 1, 3, and the local moments and diagonal-cell integrals behind
+      them (_compute_moments_sym, _triang_sym / _triang_pqpq).
+    * neon (the Z=10 ion, ns = 40 < SEMISEPARABLE_DIRECT_NS): 4-orbital keys
+      through compute_slater_rk_cell (full-bank path) and
+      compute_slater_rk_cell_batch; build_slater_rk_bilinear for one pair and
+      compute_slater_rk_table over the four spinors; compute_direct_potential_cell
+      and compute_exchange_matrix_cell at k = 0..2 (whole matrices at k = 1,
+      seeded bra/ket projections at every k); the DBSR Fock blocks of
+      DFSolver._build_hf_matrix_dbsr (methods/dirac_fock.py:1128) run
+      unmodified on a stand-in ``self`` with seeded angular coefficients.
+    * ytterbium (the Z=70 ion, ns = 120 >= SEMISEPARABLE_DIRECT_NS, whose scalar
+      path is the factored one): seeded keys through compute_slater_rk_cell
+      and compute_slater_rk_cell_batch, a bilinear table over 24 spinors, and
+      projections of the direct and exchange matrices.
+    """
+    from types import MethodType, SimpleNamespace
+
+    from atomx.methods.dirac_fock import DFSolver
+    from atomx.numerics.bspline import convol as C
+
+    from atomx_b200 import basis, workloads as W
+    from atomx_b200.angular import exchange_k_range
+
+    out = {}
+    # --------------------------------------------------------------- tiny
+    t = basis.make_exponential_knots(14, 5, 1e-4, 20.0)
+    bd = basis.prepare_bspline_data(t, 14, 5, n_gauss=6, kinetic_balance=True)
+    out["tiny_t"] = t
+    out.update({f"tiny_{k}": int(bd[k]) for k in ("nv", "ks", "ksp", "ksq", "nsp", "nsq", "ns")})
+    cache = C.ConvolCache(bd)
+    for k in (0, 1, 3):
+        for itype in ("pppp", "qqqq", "pqpq", "qpqp"):
+            rkb, ns, ks = cache.get_rkb(k, itype)
+            out[f"tiny_rkb_{itype}_{k}"] = rkb
+        for comp, ksx, b in (("p", bd["ksp"], bd["bsp_p"]), ("q", bd["ksq"], bd["bsp_q"])):
+            out[f"tiny_rising_{comp}_{k}"] = C._compute_moments_sym(b, bd["gr"], bd["grw"], bd["nv"], ksx, k)
+            out[f"tiny_falling_{comp}_{k}"] = C._compute_moments_sym(b, bd["gr"], bd["grw"], bd["nv"], ksx, -(k + 1))
+        out[f"tiny_diag_pppp_{k}"] = C._triang_sym(bd["bsp_p"], bd["gr"], bd["grw"], bd["tp"], bd["nv"], bd["ksp"],
+                                                   bd["ns"], k)
+        out[f"tiny_diag_pqpq_{k}"] = C._triang_pqpq(bd["bsp_p"], bd["bsp_q"], bd["gr"], bd["grw"], bd["tp"], bd["t"],
+                                                    bd["nv"], bd["ksp"], bd["ksq"], bd["ns"], k)
+    cache.release_shared_banks()
+
+    def keys_of(kappa, picks, rng, n_keys):
+        keys = []
+        while len(keys) < n_keys:
+            a, b, c, d = (int(x) for x in rng.choice(picks, 4))
+            ks = sorted(set(exchange_k_range(int(kappa[a]), int(kappa[b])))
+                        & set(exchange_k_range(int(kappa[c]), int(kappa[d]))))
+            if ks:
+                keys.append((a, b, c, d, int(rng.choice(ks))))
+        return np.array(keys, dtype=np.int64)
+
+    def projections(ion, cache, name, ks_, rng):
+        bd = ion.bsp
+        ns = bd["ns"]
+        vecs = rng.normal(size=(6, 2, ns))
+        jp, kp = [], []
+        for k in ks_:
+            for o in range(min(3, ion.P.shape[0])):
+                J = C.compute_direct_potential_cell(ion.P[o], ion.Q[o], bd, k, cache=cache)
+                K = C.compute_exchange_matrix_cell(ion.P[o], ion.Q[o], ion.P[o], ion.Q[o], bd, k, cache=cache)
+                a, b = vecs[2 * o], vecs[2 * o + 1]
+                jp.append((k, o, a[0] @ J[0] @ b[0], a[1] @ J[1] @ b[1]))
+                kp.append((k, o, a[0] @ K[0] @ b[0], a[1] @ K[1] @ b[1], a[0] @ K[2] @ b[1], a[1] @ K[3] @ b[0]))
+        out[f"{name}_proj_vecs"] = vecs
+        out[f"{name}_direct_proj"] = np.array(jp)
+        out[f"{name}_exchange_proj"] = np.array(kp)
+
+    # --------------------------------------------------------------- neon
+    ion = W.build_ion(W.neon_small())
+    bd = ion.bsp
+    cache = C.ConvolCache(bd)
+    od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
+    rng = np.random.default_rng(2024)
+    keys = []
+    for a in range(4):
+        for b in range(4):
+            for c in range(4):
+                for d in range(4):
+                    ks = sorted(set(exchange_k_range(int(ion.kappa[a]), int(ion.kappa[b])))
+                                & set(exchange_k_range(int(ion.kappa[c]), int(ion.kappa[d]))))
+                    keys += [(a, b, c, d, k) for k in ks if k <= 2]
+    keys = np.array(keys, dtype=np.int64)
+    out["neon_keys"] = keys
+    out["neon_cell"] = np.array([C.compute_slater_rk_cell(*od[a], *od[b], *od[c], *od[d], bd, int(k), cache=cache)
+                                 for a, b, c, d, k in keys])
+    out["neon_batch"] = np.array(C.compute_slater_rk_cell_batch(od, [tuple(int(x) for x in kk) for kk in keys], bd,
+                                                                cache=cache))
+    M = C.build_slater_rk_bilinear(ion.P[0], ion.Q[0], ion.P[1], ion.Q[1], bd, 1, cache=cache)
+    for name, m in zip(("PP", "QQ", "PQ", "QP"), M):
+        out[f"neon_bilinear_{name}"] = m
+    out["neon_bilinear_table"] = C.compute_slater_rk_table(M, ion.P.T, ion.Q.T, ion.P.T, ion.Q.T)
+    J = C.compute_direct_potential_cell(ion.P[1], ion.Q[1], bd, 1, cache=cache)
+    K = C.compute_exchange_matrix_cell(ion.P[1], ion.Q[1], ion.P[2], ion.Q[2], bd, 1, cache=cache)
+    out["neon_direct_PP"], out["neon_direct_QQ"] = J
+    for name, m in zip(("PP", "QQ", "PQ", "QP"), K):
+        out[f"neon_exchange_{name}"] = m
+    projections(ion, cache, "neon", (0, 1, 2), rng)
+    # DBSR Fock blocks on a stand-in solver: only the attributes the method reads
+    n = ion.P.shape[0]
+    kmax = 2
+    ad = rng.uniform(-1.0, 1.0, size=(n, n, kmax + 1)) * (rng.random((n, n, kmax + 1)) < 0.7)
+    ax = rng.uniform(-1.0, 1.0, size=(n, n, kmax + 1)) * (rng.random((n, n, kmax + 1)) < 0.7)
+    norms = rng.uniform(0.5, 2.0, size=n)
+    shells = [SimpleNamespace(kappa=int(x)) for x in ion.kappa]
+    me = SimpleNamespace(bsp_data=bd, subshells=shells, _angular_direct=ad, _angular_exchange=ax,
+                         _angular_k_for_target=[tuple(range(kmax + 1))] * n)
+    me._mean_field_divisor = lambda i: float(norms[i])
+    orbitals = {}
+    for i, kappa in enumerate(ion.kappa):
+        orbitals.setdefault(int(kappa), []).append((ion.P[i], ion.Q[i], 1.0))
+    hf = []
+    for target in range(n):
+        for skip in (False, True):
+            hf.append(np.stack(DFSolver._build_hf_matrix_dbsr(me, target, orbitals, skip_pq_exchange=skip)))
+    out["neon_hf_angular_direct"], out["neon_hf_angular_exchange"], out["neon_hf_norms"] = ad, ax, norms
+    out["neon_hf"] = np.array(hf)  # (target, skip) -> PP, QQ, PQ, QP
+    cache.release_shared_banks()
+
+    # ---------------------------------------------------------- ytterbium
+    ion = W.build_ion(W.ytterbium_scaleup())
+    bd = ion.bsp
+    cache = C.ConvolCache(bd)
+    od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
+    rng = np.random.default_rng(70)
+    picks = np.arange(0, 200, 9)[:24]
+    keys = keys_of(ion.kappa, picks, rng, 160)
+    keys = keys[np.isin(keys[:, 4], [0, 1, 2, 5, 12])][:96]
+    out["yb_keys"] = keys
+    out["yb_cell"] = np.array([C.compute_slater_rk_cell(*od[a], *od[b], *od[c], *od[d], bd, int(k), cache=cache)
+                               for a, b, c, d, k in keys])
+    out["yb_batch"] = np.array(C.compute_slater_rk_cell_batch(od, [tuple(int(x) for x in kk) for kk in keys], bd,
+                                                              cache=cache))
+    M = C.build_slater_rk_bilinear(ion.P[0], ion.Q[0], ion.P[9], ion.Q[9], bd, 2, cache=cache)
+    cols = picks
+    out["yb_table_cols"] = cols
+    out["yb_bilinear_table"] = C.compute_slater_rk_table(M, ion.P[cols].T, ion.Q[cols].T, ion.P[cols].T,
+                                                         ion.Q[cols].T)
+    projections(ion, cache, "yb", (0, 2), rng)
+    cache.release_shared_banks()
+    np.savez_compressed(os.path.join(HERE, "convol.npz"), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--atomx-src", required=True)
-    ap.add_argument("--only", choices=["grid", "direct", "exchange"], default=None,
+    ap.add_argument("--only", choices=["grid", "direct", "exchange", "convol"], default=None,
                     help="write only one fixture family (the others are left as they are)")
     args = ap.parse_args()
     sys.path.insert(0, args.atomx_src)
@@ -195,6 +349,10 @@ def main():
     if args.only == "direct":
         direct_potential()
         print("golden direct-potential fixtures written to", HERE)
+        return
+    if args.only == "convol":
+        convol_fixtures()
+        print("golden cell-engine fixtures written to", HERE)
         return
     if args.only == "exchange":
         exchange_matrix()
