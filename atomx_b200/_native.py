@@ -49,11 +49,24 @@ _SIGNATURES = {
     "rkb_occupied_density": [_vp, _vp, _l, _l, _vp, _l, _l, _vp, _vp],
     "rkb_bspline_sym_matrix": [_vp, _i, _vp, _i, _i, _i, _vp, _vp, _l, _vp, _vp],
     "rkb_exchange_matrix": [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp],
+    "rkb_gauss_legendre_01": [_i, _vp, _vp],
+    "rkb_cell_moments": [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp],
+    "rkb_cell_diag": [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _i, _vp, _vp],
+    "rkb_cell_assemble": [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp, _l, _l, _l, _vp],
+    "rkb_cell_densities": [_vp, _vp, _l, _vp, _l, _i, _i, _i, _i, _i, _vp, _l, _l, _vp],
+    "rkb_gemm_nt_fp64": [_vp, _l, _vp, _l, _vp, _l, _l, _l, _l, _i, _vp],
+    "rkb_cell_dots": [_vp, _l, _vp, _l, _l, _vp, _vp, _l, _vp, _vp],
+    "rkb_cell_exchange": [_vp, _l, _vp, _vp, _l, _i, _i, _i, _i, _i, _vp, _vp],
+    "rkb_cell_bilinear": [_vp, _l, _i, _vp, _vp, _i, _i, _i, _i, _i, _vp, _vp, _vp],
+    "rkb_cell_direct_density": [_vp, _l, _i, _vp, _l, _vp, _l, _i, _i, _vp, _l, _vp],
+    "rkb_cell_exchange_density": [_vp, _vp, _l, _i, _vp, _l, _l, _i, _vp, _vp],
+    "rkb_cell_banded_to_full": [_vp, _i, _i, _l, _vp, _vp],
+    "rkb_cell_fock_finish": [_vp, _vp, _i, _i, _l, _vp, _vp],
     "rkb_split_contract": [_vp, _vp, _l, _l, _i, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _vp,
                            _vp, _vp, _vp, _l, _vp, _vp, _vp],
 }
 _RESTYPE = {"rkb_last_error": _c.c_char_p, "rkb_version": _c.c_char_p, "rkb_split_fused_body_width": _c.c_long,
-            "rkb_green_factor": _c.c_long}
+            "rkb_green_factor": _c.c_long, "rkb_gauss_legendre_01": None}
 
 _lock = threading.Lock()
 _lib = None

@@ -10,6 +10,7 @@
 // through shared memory by a 3-deep cp.async ring.  One persistent CTA per SM
 // walks a host-built task list (group, tile_i, tile_j).
 #include "rkb_common.cuh"
+#include "rkb_dmma.cuh"
 
 namespace rkb {
 namespace fp64tab {
@@ -18,19 +19,6 @@ constexpr int BM = 128, BN = 128, BK = 16, PAD = 4, LDS = BK + PAD, STAGES = 3;
 constexpr int THREADS = 256;  // 8 warps as 2 (M) x 4 (N); warp tile 64 x 32
 constexpr size_t SMEM = (size_t)STAGES * (BM + BN) * LDS * sizeof(double);
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
-__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
 
 // Stage rows [row0, row0+128) x cols [k0, k0+BK) of a row-major (nrows x ld)
 // matrix into smem (128 x LDS); rows past nrows are zero-filled.

@@ -315,6 +315,82 @@ int rkb_split_certify(const long *d_grp_row0, const long *d_grp_n, long n_groups
                       const double *d_cbound, double limit, double *d_est, int *d_flagged, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Cell (bank) R^k engine: atomx numerics/bspline/convol.py (the DBSR_HF cell
+ * algorithm of the CI, MBPT and Dirac-Fock Fock-matrix paths).
+ *
+ * A bank of one component pair (left x, right y, orders ks_l, ks_r) holds
+ * rkb[i][j][ip][jp] (convol.py:1507 ConvolCache.get_rkb); on the device it is
+ * stored as the matrix K[(ip*ns + i)][(jp*ns + j)] = rkb[i][j][ip][jp] at a
+ * (row, column) offset of a caller-owned block matrix of leading dimension ld.
+ * Moments are (kk, nv) with kk = ks (ks+1)/2 packed upper pairs (i <= j);
+ * diagonal cells are (kk_l, kk_r, nv).  Banks built this way equal atomx's
+ * bit for bit.
+ *
+ * rkb_gauss_legendre_01: host only; the n-point Gauss-Legendre rule on [0, 1]
+ *   by Newton's iteration on the Legendre recurrence (convol.py:253
+ *   _gauss_legendre_01), the sub-quadrature of the diagonal cells.
+ * rkb_cell_moments: sum_m grw gr^k B_i B_j per cell, k < 0 meaning
+ *   grw / gr^-k (convol.py:58 _compute_moments_sym); bsp is (nv, ng, ks).
+ * rkb_cell_diag: the diagonal-cell integrals with an n_sub-point inner rule
+ *   (x01, w01 on [0, 1]): same != 0 is _triang_sym (convol.py:136, knots t_l =
+ *   t_r), same == 0 is _triang_pqpq (convol.py:388).
+ * rkb_cell_assemble: the bank from the left/right rising (r^k) and falling
+ *   (r^-(k+1)) moments and the diagonal cells (convol.py:324, :533).
+ * rkb_cell_densities: banded pair densities of _density_sym (convol.py:713)
+ *   for pairs (d_pairs[2p], d_pairs[2p+1]) of rows of c1, c2 (stored lengths
+ *   n1, n2 <= ld; extent ns_d <= ns_k) into out[p*out_ld + col_off + s*ns_k + i].
+ * rkb_gemm_nt_fp64: C (+)= A B^T in FP64 on the DMMA pipe (K a multiple of 16,
+ *   A and B 16-byte aligned with even leading dimensions): the pair potentials
+ *   W = D K^T of batched cell integrals (convol.py:2084) and the table GEMMs
+ *   of compute_slater_rk_table (convol.py:1988).
+ * rkb_cell_dots: out[e] = L[il[e]] . W[iw[e]] over n columns (one integral
+ *   per entry: the trace of _sum_amb_banded, convol.py:1349).
+ * rkb_cell_exchange: _convol_case4_t (convol.py:1001) for nbatch densities
+ *   (ns x ns each) on the bank blocks at K + kofs[b]; symmetric computes the
+ *   lower triangle and mirrors it; accumulate adds into out.
+ * rkb_cell_bilinear: _rkb_bilinear (convol.py:1901) on one bank block: T
+ *   scratch (ns_out * n_right * ks_r doubles) and M (ns_out x ns_out).
+ * rkb_cell_direct_density / rkb_cell_exchange_density: the density sums of
+ *   DFSolver._build_hf_matrix_dbsr (methods/dirac_fock.py:1128 with
+ *   convol.py:647 / :689) for nbatch coefficient rows (coef + b*coef_stride):
+ *   banded (ks x ns rows at out + b*out_ld, source j = target[b] doubled) and
+ *   full (ns x ns).
+ * rkb_cell_banded_to_full: V[i][i+s] += v[s*ns + i] and its mirror
+ *   (convol.py:815 _banded_to_full_add), nbatch (v, V) pairs.
+ * rkb_cell_fock_finish: the symmetrisation and norm division closing
+ *   _build_hf_matrix_dbsr (dirac_fock.py:1295-1319) on nbatch sets of
+ *   (PP, QQ, PQ, QP) blocks; out must not alias h.
+ * ------------------------------------------------------------------------- */
+void rkb_gauss_legendre_01(int n, double *x, double *w);
+int rkb_cell_moments(const double *d_bsp, const double *d_gr, const double *d_grw, int nv, int ng, int ks, int k,
+                     double *d_out, void *stream);
+int rkb_cell_diag(const double *d_bsp_l, const double *d_bsp_r, const double *d_gr, const double *d_grw,
+                  const double *d_t_l, const double *d_t_r, int nv, int ng, int ks_l, int ks_r, int same, int k,
+                  const double *d_x01, const double *d_w01, int n_sub, double *d_out, void *stream);
+int rkb_cell_assemble(const double *d_rising_l, const double *d_falling_l, const double *d_rising_r,
+                      const double *d_falling_r, const double *d_diag, int nv, int ks_l, int ks_r, int ns,
+                      double *d_out, long ld, long row_off, long col_off, void *stream);
+int rkb_cell_densities(const double *d_c1, const double *d_c2, long ld, const long *d_pairs, long n_pairs, int n1,
+                       int n2, int ns_d, int ns_k, int ks, double *d_out, long out_ld, long col_off, void *stream);
+int rkb_gemm_nt_fp64(const double *d_A, long lda, const double *d_B, long ldb, double *d_C, long ldc, long M, long N,
+                     long K, int accumulate, void *stream);
+int rkb_cell_dots(const double *d_L, long l_ld, const double *d_W, long w_ld, long n, const long *d_il,
+                  const long *d_iw, long n_ent, double *d_out, void *stream);
+int rkb_cell_exchange(const double *d_K, long ld, const long *d_kofs, const double *d_dens, long nbatch, int ns,
+                      int ks_l, int ks_r, int symmetric, int accumulate, double *d_out, void *stream);
+int rkb_cell_bilinear(const double *d_K, long ld, int ns, const double *d_wa, const double *d_wb, int n_left,
+                      int n_right, int ks_l, int ks_r, int ns_out, double *d_T, double *d_M, void *stream);
+int rkb_cell_direct_density(const double *d_comp, long ld, int n_orb, const double *d_coef, long coef_stride,
+                            const int *d_target, long nbatch, int ns, int ks, double *d_out, long out_ld,
+                            void *stream);
+int rkb_cell_exchange_density(const double *d_comp_ii, const double *d_comp_jj, long ld, int n_orb,
+                              const double *d_coef, long coef_stride, long nbatch, int ns, double *d_out,
+                              void *stream);
+int rkb_cell_banded_to_full(const double *d_v, int ns, int ks, long nbatch, double *d_V, void *stream);
+int rkb_cell_fock_finish(const double *d_h, const double *d_norm, int ns, int skip_pq, long nbatch, double *d_out,
+                         void *stream);
+
+/* ---------------------------------------------------------------------------
  * rkb_split_rows_noalloc: no counterpart in the reference (an addition of this
  * library).  The same computation and arguments as rkb_split_rows, without
  * d_xwork: the FP64 row workspace is a fixed device array inside the library,
