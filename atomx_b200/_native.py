@@ -27,6 +27,7 @@ _SIGNATURES = {
     "rkb_yk_rows": [_vp, _l, _vp, _l, _vp, _vp, _i, _i, _vp, _vp, _vp, _l, _vp],
     "rkb_eval_orbitals": [_vp, _l, _l, _vp, _i, _i, _i, _i, _vp, _l, _vp],
     "rkb_pair_density": [_vp, _vp, _l, _vp, _l, _l, _vp, _l, _vp],
+    "rkb_pack_upper": [_vp, _l, _vp, _vp],
     "rkb_weighted_dots": [_vp, _l, _vp, _l, _vp, _l, _vp, _vp, _l, _vp, _vp],
     "rkb_slater_direct": [_vp, _vp, _vp, _vp, _i, _i, _i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp],
     "rkb_grid_yk_rows": [_vp, _l, _vp, _l, _vp, _l, _vp, _vp, _vp, _l, _vp, _l, _l, _vp, _l, _vp],

@@ -265,6 +265,15 @@ __global__ void pair_density_kernel(const double *__restrict__ P, const double *
                                     __dmul_rn(Q[a * orb_ld + i], Q[c * orb_ld + i]));
 }
 
+// Row i of a symmetric n x n table, entries j >= i, to the packed upper
+// triangle: packed[i*n - i(i-1)/2 + (j - i)].  One block per row.
+__global__ void pack_upper_kernel(const double *__restrict__ T, long n, double *__restrict__ packed) {
+    const long i = blockIdx.x;
+    const double *src = T + i * n;
+    double *dst = packed + i * n - (i * (i - 1)) / 2 - i;
+    for (long j = i + threadIdx.x; j < n; j += blockDim.x) dst[j] = src[j];
+}
+
 // One warp per entry: sum_i (w_i a_i) b_i.
 __global__ void weighted_dots_kernel(const double *__restrict__ a, long a_ld, const double *__restrict__ b,
                                      long b_ld, const double *__restrict__ w, long n, const long *__restrict__ ia,
@@ -409,6 +418,14 @@ int rkb_pair_density(const double *d_P, const double *d_Q, long orb_ld, const lo
     pair_density_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, as_stream(stream)>>>(d_P, d_Q, orb_ld, d_pairs,
                                                                                        n_pairs, n, d_rho, rho_ld);
     RKB_LAUNCHED("pair_density_kernel");
+    return RKB_OK;
+}
+
+int rkb_pack_upper(const double *d_table, long n, double *d_packed, void *stream) {
+    RKB_CHECK_ARG(n >= 0 && n <= 0x7fffffffL, "invalid table size %ld", n);
+    if (n == 0) return RKB_OK;
+    pack_upper_kernel<<<(unsigned)n, 256, 0, as_stream(stream)>>>(d_table, n, d_packed);
+    RKB_LAUNCHED("pack_upper_kernel");
     return RKB_OK;
 }
 

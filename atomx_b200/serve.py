@@ -44,7 +44,12 @@ from .split import host_tables
 from .split_plan import moduli_needed
 from .tables import upload_ion
 
-__all__ = ["Request", "ServeReport", "SlaterServer", "ChecksumSink", "footprint_bytes"]
+__all__ = ["Request", "ServeReport", "SlaterServer", "ChecksumSink", "footprint_bytes", "P99_BOUND_MS"]
+
+#: The latency bound the loop is held to on the mixed-ion stream (Poisson
+#: arrivals at 200 requests/s, Z 2..92, 30..200 B-splines, 10..300 spinors,
+#: k_max 2..14): the 99th percentile of (last table delivered - arrival).
+P99_BOUND_MS = 1000.0
 
 
 @dataclass

@@ -408,12 +408,24 @@ class SplitEngine:
         """Residue position of every column of the row [X | Z] of multipole k."""
         return self.ion_rows.column_positions(k)
 
+    #: when a list, rows() appends a (start, end) CUDA event pair around the
+    #: row kernels, recorded on the launch stream
+    row_events = None
+
     def rows(self, stream=None) -> None:
         """Row kernels, then the certificate of every table (both async)."""
         self._stream = stream
+        ev = None
+        if self.row_events is not None:
+            s = stream if stream is not None else torch.cuda.current_stream()
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record(s)
         self.ion_rows.launch(self.bits, self.n_mod, self._mod_c[0], self.resA, self.resB, self.kpad, 0,
                              self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp,
                              self.xwork, stream)
+        if ev is not None:
+            ev[1].record(s)
+            self.row_events.append(ev)
         certify(self.grp_row0, self.grp_n, self.rowscale, self.cbound, self.cert_limit, self.est, self.status,
                 stream)
 
@@ -476,6 +488,12 @@ class SplitEngine:
             buf = bufs[gi % 2][:nk * nk]
             if k in fp64:
                 self._recompute(((k, 0),)).run(buf, s)
+            elif self.kernel_events is not None:
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(s)
+                self._contract(self.grp_out_zero, t0, t1, buf, s)
+                b.record(s)
+                self.kernel_events.append((a, b, k))
             else:
                 self._contract(self.grp_out_zero, t0, t1, buf, s)
             sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
@@ -484,16 +502,19 @@ class SplitEngine:
         if check:
             self.check_status()
 
-    def run_to_host(self, host: torch.Tensor, stream=None, copy_stream=None) -> None:
+    def run_to_host(self, host: torch.Tensor, stream=None, copy_stream=None, packed: bool = False) -> None:
         """The whole table into ``host`` (pinned, ``total`` doubles): the rows
         and the certificate, then each multipole's table is contracted (or
         recomputed in FP64 when its certificate failed) on ``stream`` and copied
         to the host on ``copy_stream`` while the next one is contracted.
+        ``packed``: each table's upper triangle only, at the packed offsets
+        of tables.packed_offsets (unique_entries doubles in all).
         Returns once the host copy is complete; raises like check_status()."""
         if self.out is None:
             raise ValueError("this engine streams its tables (materialize=False); use stream_tables()")
-        if host.numel() < self.total or host.is_cuda:
-            raise ValueError(f"host buffer must be a CPU tensor of at least {self.total} doubles")
+        need = self.dev.plan.unique_entries if packed else self.total
+        if host.numel() < need or host.is_cuda:
+            raise ValueError(f"host buffer must be a CPU tensor of at least {need} doubles")
         s = stream if stream is not None else torch.cuda.current_stream()
         cs = copy_stream if copy_stream is not None else self.__dict__.setdefault(
             "_copy_stream", torch.cuda.Stream(device=self.out.device))
@@ -502,6 +523,8 @@ class SplitEngine:
         _, (_, flagged) = read_status(self.status, s)  # which tables go to FP64: one wait
         fp64 = set(self._failing(self.est.cpu().numpy())) if flagged else set()
         self.escalated = sorted(fp64)
+        from .tables import PackedShipper
+        shipper = PackedShipper(plan, host, self.out.device, cs) if packed else None
         for gi, k in enumerate(plan.ks):
             nk, o = plan.n_of_k(k), self.offsets[k]
             if k in fp64:
@@ -509,6 +532,9 @@ class SplitEngine:
             else:
                 t0, t1 = self.task_range[gi]
                 self._contract(self.grp_out, t0, t1, self.out, s)
+            if shipper is not None:
+                shipper.ship(k, self.out.data_ptr() + 8 * o, s)
+                continue
             ev = torch.cuda.Event()
             ev.record(s)
             cs.wait_event(ev)
@@ -569,6 +595,30 @@ class SplitEngine:
                 "device_bytes": self.device_bytes(),
                 "tasks": self.n_tasks}
 
+    def int8_ops(self, ks=None) -> tuple[float, float]:
+        """(algorithmic, issued) int8 tensor ops of the contraction of the
+        multipoles ``ks`` (all by default): 2 * kdim ops per modulus for every
+        unique entry (i <= j) of every table; the tiles actually issued also
+        cover the lower half of diagonal tiles and the padding of edge tiles."""
+        plan = self.dev.plan
+        ops, issued = 0.0, 0.0
+        for k in (plan.ks if ks is None else ks):
+            nk = plan.n_of_k(k)
+            nt = (nk + 127) // 128
+            ops += 2.0 * self.n_mod * self.kdim[k] * (nk * (nk + 1) // 2)
+            issued += 2.0 * self.n_mod * self.kdim[k] * (nt * (nt + 1) // 2) * 128 * 128
+        return ops, issued
+
+    def row_bytes(self) -> int:
+        """Algorithmic HBM bytes of the row kernels: the orbital values read
+        once, the int8 residue matrices (and their Z-negated copy) and the
+        per-row scale, core vectors and row records written."""
+        d = self.dev
+        reads = (d.Pv.numel() + d.Qv.numel()) * 8
+        res = self.n_mod * self.dev.plan.n_rows * self.kpad * (2 if self.resB is not None else 1)
+        per_row = 8 + 2 * 8 * self.cwp + 8 * 8
+        return int(reads + res + self.dev.plan.n_rows * per_row)
+
     def roofline(self, stream=None, flush=None, reps: int = 3, kernel_ms: float | None = None) -> dict:
         """Roofline of the dominant kernel (K3s): its duration ``kernel_ms``
         (e.g. the mean of the launches recorded through ``kernel_events``
@@ -592,15 +642,7 @@ class SplitEngine:
         else:
             ms = float(kernel_ms)
         plan = self.dev.plan
-        # algorithmic work: 2 * kdim int8 ops per modulus for every unique
-        # entry (i <= j) of every table; the tiles actually issued also cover
-        # the lower half of diagonal tiles and the padding of edge tiles
-        ops, issued = 0.0, 0.0
-        for k in plan.ks:
-            nk = plan.n_of_k(k)
-            nt = (nk + 127) // 128
-            ops += 2.0 * self.n_mod * self.kdim[k] * (nk * (nk + 1) // 2)
-            issued += 2.0 * self.n_mod * self.kdim[k] * (nt * (nt + 1) // 2) * 128 * 128
+        ops, issued = self.int8_ops()
         root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
         peaks_path = os.path.join(root, "MEASURED_PEAKS.json")
         if os.path.exists(peaks_path):

@@ -27,7 +27,7 @@ from .device import as_device, resident
 from .plan import TablePlan, make_plan
 from .yk import yk_partial_matrices
 
-__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "upload_ion", "upload_values", "slater_rk_tables",
+__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "HostPackedTables", "PackedShipper", "packed_offsets", "upload_ion", "upload_values", "slater_rk_tables",
            "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE",
            "Fp64Recompute", "fp64_tables_to_host"]
 
@@ -167,6 +167,93 @@ class RkTables:
         return self.plan.ordered_entries
 
 
+def packed_offsets(plan: TablePlan) -> dict:
+    """k -> start of the k-th table in the packed (upper-triangle) layout."""
+    offs, pos = {}, 0
+    for k in plan.ks:
+        n = plan.n_of_k(k)
+        offs[k] = pos
+        pos += n * (n + 1) // 2
+    return offs
+
+
+@dataclass
+class HostPackedTables:
+    """R^k tables in pinned host memory, each stored once as its packed upper
+    triangle (the table is symmetric: R^k(ac;bd) = R^k(bd;ac)), so the
+    device-to-host copy carries every ordered entry in half the bytes.
+    ``table(k)`` expands one table; ``entry`` reads one value."""
+    plan: TablePlan
+    ks: list
+    values: torch.Tensor          # CPU (pinned), unique entries of every table
+    offsets: dict                 # k -> start in ``values`` (packed_offsets)
+    precision: str
+    info: dict = field(default_factory=dict)
+
+    def packed(self, k: int) -> np.ndarray:
+        n = self.plan.n_of_k(k)
+        o = self.offsets[k]
+        return self.values[o:o + n * (n + 1) // 2].numpy()
+
+    def table(self, k: int) -> np.ndarray:
+        n = self.plan.n_of_k(k)
+        iu = np.triu_indices(n)
+        full = np.empty((n, n))
+        v = self.packed(k)
+        full[iu] = v
+        full[(iu[1], iu[0])] = v
+        return full
+
+    def entry(self, k: int, ac: tuple, bd: tuple) -> float:
+        pk = self.plan.pairs_of_k[k]
+        pos = {tuple(self.plan.pairs[p]): i for i, p in enumerate(pk)}
+        i, j = sorted((pos[tuple(sorted(ac))], pos[tuple(sorted(bd))]))
+        n = self.plan.n_of_k(k)
+        return float(self.values[self.offsets[k] + i * n - i * (i - 1) // 2 + (j - i)])
+
+    @property
+    def ordered_entries(self) -> int:
+        return self.plan.ordered_entries
+
+    @property
+    def unique_entries(self) -> int:
+        return self.plan.unique_entries
+
+
+class PackedShipper:
+    """Ships finished tables to a pinned host buffer in packed form: each
+    table is packed on the compute stream into one of two rotating device
+    buffers and copied on the copy stream while the next table is computed."""
+
+    def __init__(self, plan: TablePlan, host: torch.Tensor, device, copy_stream):
+        self.plan, self.host, self.cs = plan, host, copy_stream
+        self.offsets = packed_offsets(plan)
+        nmax = max((plan.n_of_k(k) * (plan.n_of_k(k) + 1) // 2 for k in plan.ks), default=1)
+        self.bufs = [torch.empty(nmax, dtype=torch.float64, device=device) for _ in range(2)]
+        self.free = [None, None]
+        self.i = 0
+
+    def ship(self, k: int, table_ptr: int, stream) -> None:
+        L = _native.load()
+        b = self.i % 2
+        self.i += 1
+        if self.free[b] is not None:
+            stream.wait_event(self.free[b])
+        n = self.plan.n_of_k(k)
+        m = n * (n + 1) // 2
+        _native.check(L.rkb_pack_upper(table_ptr, n, self.bufs[b].data_ptr(), _native.stream_handle(stream)),
+                      "rkb_pack_upper")
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        self.cs.wait_event(ev)
+        o = self.offsets[k]
+        with torch.cuda.stream(self.cs):
+            self.host[o:o + m].copy_(self.bufs[b][:m], non_blocking=True)
+            fe = torch.cuda.Event()
+            fe.record(self.cs)
+        self.free[b] = fe
+
+
 class Fp64Workspace:
     """Device buffers of the plain engine for one ion, reusable across calls."""
 
@@ -251,9 +338,10 @@ class Fp64Recompute:
 
 
 def fp64_tables_to_host(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, host: torch.Tensor, stream=None,
-                        copy_stream=None) -> None:
+                        copy_stream=None, packed: bool = False) -> None:
     """Plain FP64 engine with each multipole's table copied to ``host`` on
-    ``copy_stream`` while the next one is contracted; returns when done."""
+    ``copy_stream`` while the next one is contracted (``packed``: each
+    table's upper triangle, at packed_offsets); returns when done."""
     L = _native.load()
     s = stream if stream is not None else torch.cuda.current_stream()
     cs = copy_stream if copy_stream is not None else torch.cuda.Stream(device=out.device)
@@ -264,12 +352,16 @@ def fp64_tables_to_host(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, ho
                                         dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
                                         dev.mi.data_ptr(), ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, h),
                   "rkb_table_rows_fp64")
+    shipper = PackedShipper(plan, host, out.device, cs) if packed else None
     for gi, k in enumerate(plan.ks):
         t0, t1 = ws.task_range[gi]
         nk, o = plan.n_of_k(k), ws.offsets[k]
         _native.check(L.rkb_table_contract_fp64(ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, ws.ld, ws.row0.data_ptr(),
                                                 ws.nk.data_ptr(), ws.out_off.data_ptr(), ws.tasks.data_ptr() + 12 * t0,
                                                 t1 - t0, out.data_ptr(), h), "rkb_table_contract_fp64")
+        if shipper is not None:
+            shipper.ship(k, out.data_ptr() + 8 * o, s)
+            continue
         ev = torch.cuda.Event()
         ev.record(s)
         cs.wait_event(ev)
@@ -279,7 +371,7 @@ def fp64_tables_to_host(dev: IonDevice, ws: Fp64Workspace, out: torch.Tensor, ho
 
 
 def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", stream=None, sink=None,
-                     host: bool = False, **split_opts):
+                     host: bool = False, packed: bool = False, **split_opts):
     """All R^k tables of one ion on the device (see module docstring).
 
     With ``sink`` the tables are streamed instead of returned: the engine
@@ -294,13 +386,16 @@ def slater_rk_tables(ion, k_max: int | None = None, precision: str = "fp64", str
     With ``host=True`` the tables come back in pinned host memory
     (``values`` is a CPU tensor): each multipole's table is copied while the
     next one is contracted, so the device-to-host copy hides the compute.
+    ``packed=True`` (with ``host=True``) ships each table's upper triangle
+    only and returns a ``HostPackedTables``: every ordered entry in half the
+    bytes.
     """
     if precision not in ("fp64", "split"):
         raise ValueError(f"unknown precision {precision!r}; choose 'fp64' or 'split'")
     dev = upload_ion(ion, k_max=k_max, stream=stream)
     if sink is not None:
         return stream_tables(dev, sink, precision=precision, stream=stream, **split_opts)
-    return tables_for(dev, precision=precision, stream=stream, host=host, **split_opts)
+    return tables_for(dev, precision=precision, stream=stream, host=host, packed=packed, **split_opts)
 
 
 @dataclass
@@ -388,8 +483,25 @@ def slater_rk_tables_from_values(Pv, Qv, kappa, gr, grw, k_max: int, precision: 
     return tables_for(dev, precision=precision, stream=stream, **split_opts)
 
 
-def tables_for(dev: IonDevice, precision: str = "fp64", stream=None, host: bool = False,
-               **split_opts) -> RkTables:
+def tables_for(dev: IonDevice, precision: str = "fp64", stream=None, host: bool = False, packed: bool = False,
+               **split_opts):
+    if packed and not host:
+        raise ValueError("packed tables are a host format: pass host=True")
+    if packed:
+        plan = dev.plan
+        values = torch.empty(max(plan.unique_entries, 1), dtype=torch.float64, pin_memory=True)
+        if precision == "split":
+            from .split import SplitEngine
+            eng = SplitEngine(dev, **split_opts)
+            eng.run_to_host(values, stream=stream, packed=True)
+            info = eng.info()
+        else:
+            ws = Fp64Workspace(dev)
+            out = torch.empty(ws.total, device=dev.Pv.device, dtype=torch.float64)
+            fp64_tables_to_host(dev, ws, out, values, stream=stream, packed=True)
+            info = {}
+        return HostPackedTables(plan=plan, ks=plan.ks, values=values, offsets=packed_offsets(plan),
+                                precision=precision, info=info)
     if precision == "split":
         from .split import SplitEngine
         eng = SplitEngine(dev, **split_opts)

@@ -414,6 +414,7 @@ def run_gpu(args):
         t_wall = time.perf_counter()
         if engine == "split":
             eng.kernel_events = []  # the contraction's own launches inside the timed steps
+            eng.row_events = []     # and the row kernels
         times = _time_steps(step, args.steps, flush, stream)
         barrier(world)
         t_wall = time.perf_counter() - t_wall
@@ -427,8 +428,17 @@ def run_gpu(args):
     if engine == "split":
         torch.cuda.synchronize()
         live = [a.elapsed_time(b) for a, b in eng.kernel_events]
-        eng.kernel_events = None
+        rows_live = [a.elapsed_time(b) for a, b in eng.row_events]
+        eng.kernel_events = eng.row_events = None
         dom = eng.roofline(kernel_ms=statistics.mean(live))
+        peaks, psrc = measured_peaks()
+        rms = statistics.mean(rows_live)
+        gbs = eng.row_bytes() / (rms / 1e3) / 1e9
+        extra["row_kernels"] = {"kernel": f"split rows ({eng.ion_rows.kind})", "ms": rms,
+                                "algorithmic_bytes": eng.row_bytes(), "achieved_gbs": gbs,
+                                "peak_gbs": float(peaks["hbm_gbs"]), "frac": gbs / float(peaks["hbm_gbs"]),
+                                "peak_source": psrc, "bound": "issue (residue arithmetic), HBM below it",
+                                "timing": f"CUDA events around the row launches of the {len(rows_live)} timed steps"}
         dom["timing"] = (f"CUDA events on the launch stream around each of the {len(live)} contraction launches "
                          "inside the timed steps (mean)")
         dom["traffic"] = profiled_traffic(dom["kernel"], plan)
@@ -477,6 +487,8 @@ def run_gpu(args):
         line["batch"] = batch_leg()
     if not args.no_stream and extra_legs:
         line["stream"] = stream_leg()
+    if not args.no_cell and extra_legs:
+        line["cell"] = cell_leg()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:  # the host baseline is measured at N=1 only
         line["cpu_baseline"] = cpu_baseline(ion, plan)
     if rank == 0:
@@ -519,9 +531,10 @@ def e2e_leg(ion, engine, args, world, k_max):
     for i in range(steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        # host=True: each multipole's table is copied to pinned host memory
-        # while the next one is contracted
-        tab = T.slater_rk_tables(ion, k_max=k_max, precision=engine, host=True)
+        # host=True, packed=True: each multipole's table (its upper triangle,
+        # which holds every ordered entry of the symmetric table) is copied to
+        # pinned host memory while the next one is contracted
+        tab = T.slater_rk_tables(ion, k_max=k_max, precision=engine, host=True, packed=True)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         assert not tab.values.is_cuda
@@ -533,9 +546,10 @@ def e2e_leg(ion, engine, args, world, k_max):
     tmax = allreduce_max(float(np.median(times)), world)
     ent = allreduce_sum(float(plan.ordered_entries), world)
     return {"value": ent / tmax, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(plan.ordered_entries * 8), "steps": steps,
-            "note": "slater_rk_tables(ion, host=True) from host coefficients to the full table in pinned host "
-                    "memory, per-multipole copies overlapped with the contraction"}
+            "d2h_bytes_per_step": int(plan.unique_entries * 8), "steps": steps,
+            "note": "slater_rk_tables(ion, host=True, packed=True) from host coefficients to every table in pinned "
+                    "host memory as its packed upper triangle (all ordered entries, R(ac;bd) = R(bd;ac)), "
+                    "per-multipole copies overlapped with the contraction"}
 
 
 def serve_leg(args) -> dict:
@@ -548,8 +562,10 @@ def serve_leg(args) -> dict:
     stream = W.serving_requests(n_requests=args.serve)
     with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
         ions = list(ex.map(lambda ts: W.build_ion(ts[1]), stream))  # client-side data, not timed
+    from atomx_b200.serve import P99_BOUND_MS
     out = {"requests": len(stream), "rate_per_s": 200.0, "arrival_span_s": stream[-1][0],
            "sink": "device: per-(k, row) sums of every multipole table",
+           "p99_bound_ms": P99_BOUND_MS,
            "note": "latency = last table delivered - arrival (server clock), realtime Poisson arrivals"}
     for precision in ("split", "fp64"):
         reqs = [Request(rid=i, ion=ion, k_max=spec.k_max, arrival=t)
@@ -558,11 +574,12 @@ def serve_leg(args) -> dict:
         warm.serve([Request(rid=-1, ion=ions[0], k_max=stream[0][1].k_max)], realtime=False)
         warm.close()
         torch_sync()
-        server = SlaterServer(precision=precision, max_inflight=4)
+        server = SlaterServer(precision=precision, max_inflight=args.serve_slots, workers=8)
         rep = server.serve(reqs, realtime=True)
         server.close()
         torch_sync()
         out[precision] = rep.summary()
+        out[precision]["within_p99_bound"] = out[precision]["p99_ms"] <= P99_BOUND_MS
         errs = [repr(r.error) for r in reqs if r.error is not None]
         if errs:
             out[precision]["errors"] = errs[:3]
@@ -677,7 +694,146 @@ def stream_leg(reps: int = 2) -> dict:
             out[precision]["bits"], out[precision]["rows_kernel"] = info.get("bits"), info.get("rows_kernel")
         torch.cuda.empty_cache()
     out["speedup_split_vs_fp64"] = out["fp64"]["ms"] / out["split"]["ms"]
+    out.update(stream_diagnostics(dev, s))
     return out
+
+
+def stream_diagnostics(dev, s) -> dict:
+    """One more streamed pass of each engine, instrumented (not the timed
+    passes): the split table's error against the plain FP64 table for every
+    multipole (Schwarz-relative, floored-relative, absolute), the
+    contraction's int8 tensor-pipe rate from CUDA events around each of its
+    launches, and the row kernels' algorithmic HBM rate."""
+    import torch
+
+    from atomx_b200 import tables as T
+    from atomx_b200.split import SplitEngine
+    plan = dev.plan
+    ref = {}
+
+    def keep(k, table, blocks, stream):
+        with torch.cuda.stream(stream):
+            ref[k] = table.clone()
+
+    T.stream_tables(dev, keep, precision="fp64", stream=s)
+    torch.cuda.synchronize()
+    errs = {}
+
+    def compare(k, table, blocks, stream):
+        with torch.cuda.stream(stream):
+            r = ref[k]
+            d = (table - r).abs()
+            dg = r.diagonal().abs().sqrt()
+            floor = 1e-6 * float(r.abs().max())
+            errs[str(k)] = {"schwarz_rel": _nan_inf(float((d / torch.outer(dg, dg)).max())),
+                            "rel_floored_1e-6": _nan_inf(float((d / r.abs().clamp_min(floor)).max())),
+                            "abs": _nan_inf(float(d.max()))}
+
+    eng = SplitEngine(dev, materialize=False)
+    eng.kernel_events, eng.row_events = [], []
+    eng.stream_tables(compare, stream=s)
+    torch.cuda.synchronize()
+    del ref
+    torch.cuda.empty_cache()
+    ops = ms = 0.0
+    for a, b, k in eng.kernel_events:
+        ms += a.elapsed_time(b)
+        ops += eng.int8_ops([k])[0]
+    rms = sum(a.elapsed_time(b) for a, b in eng.row_events)
+    peaks, src = measured_peaks()
+    tops = ops / (ms / 1e3) / 1e12
+    gbs = eng.row_bytes() / (rms / 1e3) / 1e9
+    return {"error_vs_fp64": {"max_schwarz_rel": max(e["schwarz_rel"] for e in errs.values()),
+                              "max_rel_floored_1e-6": max(e["rel_floored_1e-6"] for e in errs.values()),
+                              "max_abs": max(e["abs"] for e in errs.values()), "per_table": errs,
+                              "tables_recomputed_fp64": list(eng.escalated)},
+            "contraction": {"kernel": eng.dominant_kernel, "ms": ms, "int8_tops": tops,
+                            "peak_tops": 2.0 * float(peaks["bf16_tflops"]),
+                            "frac": tops / (2.0 * float(peaks["bf16_tflops"])), "peak_source": src,
+                            "timing": "CUDA events around each multipole's contraction launch"},
+            "row_kernels": {"kind": eng.ion_rows.kind, "ms": rms, "algorithmic_bytes": eng.row_bytes(),
+                            "achieved_gbs": gbs, "frac_of_hbm": gbs / float(peaks["hbm_gbs"])}}
+
+
+def cell_leg(reps: int = 3, cpu_keys: int = 256) -> dict:
+    """The cell (bank) engine of atomx convol.py on the Z=70 ion: every
+    allowed R^k(ac;bd), k <= 12, as whole cell tables (3.18e8 ordered
+    entries; the banks are built once and stay on the device).  CUDA events
+    around each whole pass; the FP64 GEMMs are timed against cuBLAS DGEMM.
+    Host baseline: the oracle's cell integral (the reference's full-bank
+    path, bit-identical to atomx) on a sample of keys, one key per host
+    thread (ctypes releases the interpreter lock in the C loops)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    from atomx_b200 import convol as C
+    from atomx_b200 import workloads as W
+    from oracle import cell as OC
+    from oracle import oracle
+    spec = W.ytterbium_scaleup()
+    ion = W.build_ion(spec)
+    bd = ion.bsp
+    cache = C.ConvolCache(bd)
+    cache.release_shared_banks()
+    s = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for k in range(spec.k_max + 1):
+        cache.bank(k, s)
+    e1.record(s)
+    torch.cuda.synchronize()
+    bank_ms = e0.elapsed_time(e1)
+    P = C._stack(list(ion.P), bd["ns"], torch.device("cuda"))
+    Q = C._stack(list(ion.Q), bd["ns"], torch.device("cuda"))
+    tab = C.cell_tables(P, Q, ion.kappa, bd, spec.k_max, cache=cache)
+    plan = tab.plan
+    ts = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        tab = C.cell_tables(P, Q, ion.kappa, bd, spec.k_max, cache=cache, plan=plan)
+        b.record(s)
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    ms = statistics.median(ts)
+    kdim = cache.bank(0).kdim
+    flops = sum(2.0 * plan.n_of_k(k) * kdim * kdim + 2.0 * kdim * plan.n_of_k(k) * (plan.n_of_k(k) + 1) / 2
+                for k in plan.ks)
+    peak, psrc = fp64_peak()
+    # host: the reference algorithm's cell integral on a seeded sample of keys
+    rng = np.random.default_rng(5)
+    keys = []
+    for _ in range(cpu_keys):
+        k = int(rng.choice(plan.ks))
+        pk = plan.pairs[plan.pairs_of_k[k]]
+        (a_, c_), (b_, d_) = pk[rng.integers(len(pk))], pk[rng.integers(len(pk))]
+        keys.append((int(a_), int(c_), int(b_), int(d_), k))
+    banks = OC.Banks(bd)
+    for k in sorted({kk[4] for kk in keys}):
+        for it in OC.ITYPES:
+            banks(k, it)
+    threads = oracle.max_threads()
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        ref = list(ex.map(lambda kk: OC.slater_rk_cell(ion.P[kk[0]], ion.Q[kk[0]], ion.P[kk[1]], ion.Q[kk[1]],
+                                                        ion.P[kk[2]], ion.Q[kk[2]], ion.P[kk[3]], ion.Q[kk[3]],
+                                                        bd, kk[4], banks), keys))
+    cpu_s = time.perf_counter() - t0
+    got = np.array([tab.entry(kk[4], (kk[0], kk[1]), (kk[2], kk[3])) for kk in keys])
+    err = float(np.max(np.abs(got - np.array(ref))) / np.max(np.abs(ref)))
+    return {"workload": "ytterbium_scaleup cell tables: every allowed R^k(ac;bd), k<=12, by the bank engine "
+                        "(atomx convol.py), 120 B-splines order 9 (kdim 2048)",
+            "entries": plan.ordered_entries, "ms": ms, "integrals_per_s": plan.ordered_entries / (ms / 1e3),
+            "bank_build_ms_k0_12": bank_ms,
+            "roofline": {"bound": "tensor (FP64 DMMA)", "achieved_tflops": flops / (ms / 1e3) / 1e12,
+                         "peak_tflops": peak, "frac": flops / (ms / 1e3) / 1e12 / peak, "peak_source": psrc,
+                         "algorithmic_flops": flops},
+            "cpu_baseline": {"value": cpu_keys / cpu_s, "unit": "integrals/s", "cores": threads, "kind": "port",
+                             "sample": f"{cpu_keys} seeded keys through the oracle's full-bank cell integral"},
+            "speedup_vs_cpu": (plan.ordered_entries / (ms / 1e3)) / (cpu_keys / cpu_s),
+            "max_rel_err_vs_oracle": err}
 
 
 def batch_leg(reps: int = 3) -> dict:
@@ -751,10 +907,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
-    ap.add_argument("--serve", type=int, default=32, help="requests in the serving leg (0 = skip)")
+    ap.add_argument("--serve", type=int, default=300, help="requests in the serving leg (0 = skip)")
+    ap.add_argument("--serve-slots", type=int, default=8, help="requests on the GPU at once in the serving leg")
     ap.add_argument("--no-grid", action="store_true", help="skip the arbitrary-grid Y^k leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-ion batch leg")
     ap.add_argument("--no-stream", action="store_true", help="skip the streamed Z=54 CI table leg")
+    ap.add_argument("--no-cell", action="store_true", help="skip the cell (bank) engine leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -74,6 +74,13 @@ int rkb_eval_orbitals(const double *d_coeff, long coeff_ld, long n_orb, const do
 int rkb_pair_density(const double *d_P, const double *d_Q, long orb_ld, const long *d_pairs,
                      long n_pairs, long n, double *d_rho, long rho_ld, void *stream);
 
+/* The upper triangle (j >= i) of a symmetric n x n row-major table, packed
+ * row by row: packed[i*n - i(i-1)/2 + (j - i)] = T[i][j], n(n+1)/2 doubles.
+ * Every ordered entry of an R^k table, R^k(ac;bd) = R^k(bd;ac), is in it;
+ * the engine ships tables to the host in this form (atomx returns each
+ * integral separately, numerics/bspline/slater.py:118). */
+int rkb_pack_upper(const double *d_table, long n, double *d_packed, void *stream);
+
 /* Quadrature dots out[e] = sum_i w_i a[ia[e]]_i b[ib[e]]_i (atomx
  * numerics/bspline/slater.py:130, the slater_rk_poisson contraction). */
 int rkb_weighted_dots(const double *d_a, long a_ld, const double *d_b, long b_ld,

@@ -188,6 +188,9 @@ def exchange_matrix():
 def convol_fixtures():
     """Golden vectors of atomx's cell (bank) R^k engine, numerics/bspline/convol.py.
 
+    Every input is stored with the outputs (basis arrays, coefficients), so
+    the device tests run on exactly these numbers.
+
     * tiny: a 14-spline order-5 kinetically balanced basis on which whole
       banks fit a fixture: ConvolCache.get_rkb for all four component types at
       k = 0, 1, 3, and the local moments and diagonal-cell integrals behind
@@ -214,11 +217,17 @@ def convol_fixtures():
     from atomx_b200.angular import exchange_k_range
 
     out = {}
+
+    def keep_basis(name, bd):
+        """The basis arrays themselves: a GPU host rebuilds nothing (its
+        LAPACK and vector math may round differently in the last bit)."""
+        out.update({f"{name}_{k}": np.asarray(bd[k]) for k in ("gr", "grw", "bsp_p", "bsp_q", "t", "tp")})
+        out.update({f"{name}_{k}": int(bd[k]) for k in ("nv", "ks", "ksp", "ksq", "nsp", "nsq", "ns")})
+
     # --------------------------------------------------------------- tiny
     t = basis.make_exponential_knots(14, 5, 1e-4, 20.0)
     bd = basis.prepare_bspline_data(t, 14, 5, n_gauss=6, kinetic_balance=True)
-    out["tiny_t"] = t
-    out.update({f"tiny_{k}": int(bd[k]) for k in ("nv", "ks", "ksp", "ksq", "nsp", "nsq", "ns")})
+    keep_basis("tiny", bd)
     cache = C.ConvolCache(bd)
     for k in (0, 1, 3):
         for itype in ("pppp", "qqqq", "pqpq", "qpqp"):
@@ -243,16 +252,16 @@ def convol_fixtures():
                 keys.append((a, b, c, d, int(rng.choice(ks))))
         return np.array(keys, dtype=np.int64)
 
-    def projections(ion, cache, name, ks_, rng):
+    def projections(ion, cache, name, ks_, rng, orbs):
         bd = ion.bsp
         ns = bd["ns"]
         vecs = rng.normal(size=(6, 2, ns))
         jp, kp = [], []
         for k in ks_:
-            for o in range(min(3, ion.P.shape[0])):
+            for slot, o in enumerate(orbs):
                 J = C.compute_direct_potential_cell(ion.P[o], ion.Q[o], bd, k, cache=cache)
                 K = C.compute_exchange_matrix_cell(ion.P[o], ion.Q[o], ion.P[o], ion.Q[o], bd, k, cache=cache)
-                a, b = vecs[2 * o], vecs[2 * o + 1]
+                a, b = vecs[2 * slot], vecs[2 * slot + 1]
                 jp.append((k, o, a[0] @ J[0] @ b[0], a[1] @ J[1] @ b[1]))
                 kp.append((k, o, a[0] @ K[0] @ b[0], a[1] @ K[1] @ b[1], a[0] @ K[2] @ b[1], a[1] @ K[3] @ b[0]))
         out[f"{name}_proj_vecs"] = vecs
@@ -262,6 +271,8 @@ def convol_fixtures():
     # --------------------------------------------------------------- neon
     ion = W.build_ion(W.neon_small())
     bd = ion.bsp
+    keep_basis("neon", bd)
+    out["neon_P"], out["neon_Q"], out["neon_kappa"] = ion.P, ion.Q, ion.kappa
     cache = C.ConvolCache(bd)
     od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
     rng = np.random.default_rng(2024)
@@ -288,7 +299,7 @@ def convol_fixtures():
     out["neon_direct_PP"], out["neon_direct_QQ"] = J
     for name, m in zip(("PP", "QQ", "PQ", "QP"), K):
         out[f"neon_exchange_{name}"] = m
-    projections(ion, cache, "neon", (0, 1, 2), rng)
+    projections(ion, cache, "neon", (0, 1, 2), rng, (0, 1, 2))
     # DBSR Fock blocks on a stand-in solver: only the attributes the method reads
     n = ion.P.shape[0]
     kmax = 2
@@ -313,10 +324,12 @@ def convol_fixtures():
     # ---------------------------------------------------------- ytterbium
     ion = W.build_ion(W.ytterbium_scaleup())
     bd = ion.bsp
+    keep_basis("yb", bd)
     cache = C.ConvolCache(bd)
     od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
     rng = np.random.default_rng(70)
     picks = np.arange(0, 200, 9)[:24]
+    out["yb_orbitals"], out["yb_P"], out["yb_Q"] = picks, ion.P[picks], ion.Q[picks]
     keys = keys_of(ion.kappa, picks, rng, 160)
     keys = keys[np.isin(keys[:, 4], [0, 1, 2, 5, 12])][:96]
     out["yb_keys"] = keys
@@ -329,7 +342,7 @@ def convol_fixtures():
     out["yb_table_cols"] = cols
     out["yb_bilinear_table"] = C.compute_slater_rk_table(M, ion.P[cols].T, ion.Q[cols].T, ion.P[cols].T,
                                                          ion.Q[cols].T)
-    projections(ion, cache, "yb", (0, 2), rng)
+    projections(ion, cache, "yb", (0, 2), rng, (0, 9, 18))
     cache.release_shared_banks()
     np.savez_compressed(os.path.join(HERE, "convol.npz"), **out)
 

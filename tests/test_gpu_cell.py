@@ -14,12 +14,10 @@ Gates:
   the Z=70 basis where atomx's scalar path is its factored one (which differs
   from the full bank by ~2e-12).
 """
-import os
-
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+import cell_fixtures as F
 from oracle import cell as OC
 
 pytestmark = pytest.mark.gpu
@@ -29,13 +27,25 @@ torch = pytest.importorskip("torch")
 
 @pytest.fixture(scope="module")
 def gold():
-    return np.load(os.path.join(GOLDEN, "convol.npz"))
+    return F.load()
 
 
 def _tiny(g):
-    from atomx_b200 import basis
-    return basis.prepare_bspline_data(g["tiny_t"], int(g["tiny_ns"]), int(g["tiny_ks"]), n_gauss=6,
-                                      kinetic_balance=True)
+    return F.basis(g, "tiny")
+
+
+class _Ion:
+    """The stored basis and spinors of one fixture ion (as atomx saw them)."""
+
+    def __init__(self, g, name):
+        self.bsp = F.basis(g, name)
+        od = F.orbitals(g, name)
+        n = max(od) + 1
+        self.P = np.zeros((n, self.bsp["ns"]))
+        self.Q = np.zeros((n, self.bsp["ns"]))
+        for i, (p, q) in od.items():
+            self.P[i], self.Q[i] = p, q
+        self.od = od
 
 
 def _ion(name):
@@ -70,12 +80,12 @@ def test_device_banks_bitwise_tiny(gold, k):
         assert np.array_equal(b.moments[comp, "falling"].cpu().numpy(), gold[f"tiny_falling_{comp}_{k}"])
 
 
-@pytest.mark.parametrize("name,ks_", [("neon_small", (0, 1, 2)), ("ytterbium_scaleup", (0, 5, 12))])
-def test_device_banks_bitwise_vs_oracle(name, ks_):
+@pytest.mark.parametrize("name,ks_", [("neon", (0, 1, 2)), ("yb", (0, 5, 12))])
+def test_device_banks_bitwise_vs_oracle(gold, name, ks_):
     """Whole banks of the Z=10 (ns=40) and Z=70 (ns=120) bases, every
     component pair, against the oracle restatement of atomx's builder."""
     from atomx_b200.convol import ITYPES, ConvolCache
-    bd = _ion(name).bsp
+    bd = F.basis(gold, name)
     cache = ConvolCache(bd)
     for k in ks_:
         for itype in ITYPES:
@@ -86,9 +96,8 @@ def test_device_banks_bitwise_vs_oracle(name, ks_):
 
 def test_cell_integrals_neon(gold):
     from atomx_b200 import convol as C
-    ion = _ion("neon_small")
-    bd = ion.bsp
-    od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
+    ion = _Ion(gold, "neon")
+    bd, od = ion.bsp, ion.od
     keys = [tuple(int(x) for x in kk) for kk in gold["neon_keys"]]
     got = np.array(C.compute_slater_rk_cell_batch(od, keys, bd))
     _close(got, gold["neon_cell"], 1e-13)
@@ -105,8 +114,8 @@ def test_cell_integrals_neon(gold):
 
 def test_cell_integrals_ytterbium(gold):
     from atomx_b200 import convol as C
-    ion = _ion("ytterbium_scaleup")
-    od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
+    ion = _Ion(gold, "yb")
+    od = ion.od
     keys = [tuple(int(x) for x in kk) for kk in gold["yb_keys"]]
     got = np.array(C.compute_slater_rk_cell_batch(od, keys, ion.bsp))
     _close(got, gold["yb_batch"], 1e-13)   # atomx's full-bank batch kernel
@@ -115,7 +124,7 @@ def test_cell_integrals_ytterbium(gold):
 
 def test_bilinear_and_table_neon(gold):
     from atomx_b200 import convol as C
-    ion = _ion("neon_small")
+    ion = _Ion(gold, "neon")
     M = C.build_slater_rk_bilinear(ion.P[0], ion.Q[0], ion.P[1], ion.Q[1], ion.bsp, 1)
     for name, m in zip(("PP", "QQ", "PQ", "QP"), M):
         assert np.array_equal(m, gold[f"neon_bilinear_{name}"]), name
@@ -127,7 +136,7 @@ def test_bilinear_and_table_neon(gold):
 
 def test_bilinear_table_ytterbium(gold):
     from atomx_b200 import convol as C
-    ion = _ion("ytterbium_scaleup")
+    ion = _Ion(gold, "yb")
     M = C.build_slater_rk_bilinear(ion.P[0], ion.Q[0], ion.P[9], ion.Q[9], ion.bsp, 2)
     cols = gold["yb_table_cols"]
     tab = C.compute_slater_rk_table(M, ion.P[cols].T, ion.Q[cols].T, ion.P[cols].T, ion.Q[cols].T)
@@ -136,7 +145,7 @@ def test_bilinear_table_ytterbium(gold):
 
 def test_direct_and_exchange_matrices_neon(gold):
     from atomx_b200 import convol as C
-    ion = _ion("neon_small")
+    ion = _Ion(gold, "neon")
     bd = ion.bsp
     J = C.compute_direct_potential_cell(ion.P[1], ion.Q[1], bd, 1)
     for name, m in zip(("PP", "QQ"), J):
@@ -156,12 +165,14 @@ def test_direct_and_exchange_matrices_neon(gold):
 @pytest.mark.parametrize("name,tol", [("neon", 1e-13), ("yb", 1e-11)])
 def test_direct_exchange_projections(gold, name, tol):
     from atomx_b200 import convol as C
-    ion = _ion("neon_small" if name == "neon" else "ytterbium_scaleup")
+    ion = _Ion(gold, name)
     bd = ion.bsp
     vecs = gold[f"{name}_proj_vecs"]
+    orbs = sorted({int(r[1]) for r in gold[f"{name}_direct_proj"]})
     for row_j, row_k in zip(gold[f"{name}_direct_proj"], gold[f"{name}_exchange_proj"]):
         k, o = int(row_j[0]), int(row_j[1])
-        a, b = vecs[2 * o], vecs[2 * o + 1]
+        slot = orbs.index(o)
+        a, b = vecs[2 * slot], vecs[2 * slot + 1]
         J = C.compute_direct_potential_cell(ion.P[o], ion.Q[o], bd, k)
         K = C.compute_exchange_matrix_cell(ion.P[o], ion.Q[o], ion.P[o], ion.Q[o], bd, k)
         gj = np.array([a[0] @ J[0] @ b[0], a[1] @ J[1] @ b[1]])
@@ -196,7 +207,7 @@ def test_direct_exchange_contract_to_cell_integrals():
 
 def test_dbsr_fock_blocks_neon(gold):
     from atomx_b200 import convol as C
-    ion = _ion("neon_small")
+    ion = _Ion(gold, "neon")
     n = ion.P.shape[0]
     ad, ax, norms = gold["neon_hf_angular_direct"], gold["neon_hf_angular_exchange"], gold["neon_hf_norms"]
     for s, skip in enumerate((False, True)):
@@ -230,9 +241,8 @@ def test_cell_tables_against_batch_and_poisson():
 
 def test_pair_potentials_and_radial_evaluator(gold):
     from atomx_b200 import convol as C
-    ion = _ion("neon_small")
-    bd = ion.bsp
-    od = {i: (ion.P[i], ion.Q[i]) for i in range(ion.P.shape[0])}
+    ion = _Ion(gold, "neon")
+    bd, od = ion.bsp, ion.od
     ev = C.radial_evaluator(od, bd, pair_potential_cache_size=3)
     # R^k(ac, bd): key ("r", k, a, c, b, d) equals compute_slater_rk_cell(a, c, b, d)
     keys = [("r", int(k), int(a), int(b), int(c), int(d)) for a, b, c, d, k in gold["neon_keys"][:60]]

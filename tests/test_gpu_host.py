@@ -42,3 +42,26 @@ def test_slater_rk_tables_host_flag():
     b = slater_rk_tables(ion, precision="split")
     assert torch.equal(a.values, b.values.cpu())
     assert np.isfinite(a.values.numpy()).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_packed_host_tables_equal_device_tables(precision):
+    """host=True, packed=True ships each table's upper triangle; expanded, it
+    equals the device table bit for bit (same engine, same launches)."""
+    import numpy as np
+    import torch
+
+    from atomx_b200 import workloads as W
+    from atomx_b200.tables import HostPackedTables, slater_rk_tables
+    ion = W.build_ion(W.neon_small())
+    dev = slater_rk_tables(ion, precision=precision)
+    host = slater_rk_tables(ion, precision=precision, host=True, packed=True)
+    assert isinstance(host, HostPackedTables) and not host.values.is_cuda
+    assert host.values.numel() == host.plan.unique_entries
+    for k in dev.ks:
+        assert np.array_equal(host.table(k), dev.table(k).cpu().numpy()), k
+    pr = dev.plan.pairs[dev.plan.pairs_of_k[1]]
+    assert host.entry(1, tuple(pr[0]), tuple(pr[-1])) == dev.entry(1, tuple(pr[-1]), tuple(pr[0]))
+    with pytest.raises(ValueError):
+        slater_rk_tables(ion, precision=precision, packed=True)
+    torch.cuda.synchronize()

@@ -7,24 +7,20 @@ cells, banks, the full-bank scalar path, exchange contractions); to a few
 ulps of the result's scale where atomx uses fastmath (_convol_case1_t, the
 direct density accumulation) or its factored path (ns >= 96).
 """
-import os
-
 import numpy as np
 import pytest
 
-from conftest import GOLDEN
+import cell_fixtures as F
 from oracle import cell as C
 
 
 @pytest.fixture(scope="module")
 def gold():
-    return np.load(os.path.join(GOLDEN, "convol.npz"))
+    return F.load()
 
 
 def _tiny(g):
-    from atomx_b200 import basis
-    ns, ks = int(g["tiny_ns"]), int(g["tiny_ks"])
-    return basis.prepare_bspline_data(g["tiny_t"], ns, ks, n_gauss=6, kinetic_balance=True)
+    return F.basis(g, "tiny")
 
 
 def test_gauss_legendre_01():
@@ -56,13 +52,23 @@ def test_banks_bitwise(gold, k, itype):
     assert np.array_equal(rkb, ref)
 
 
-def _neon():
-    from atomx_b200 import workloads as W
-    return W.build_ion(W.neon_small())
+class _Ion:
+    def __init__(self, g, name):
+        self.bsp = F.basis(g, name)
+        od = F.orbitals(g, name)
+        n = max(od) + 1
+        self.P = np.zeros((n, self.bsp["ns"]))
+        self.Q = np.zeros((n, self.bsp["ns"]))
+        for i, (p, q) in od.items():
+            self.P[i], self.Q[i] = p, q
+
+
+def _neon(g):
+    return _Ion(g, "neon")
 
 
 def test_scalar_cell_integrals_neon_bitwise(gold):
-    ion = _neon()
+    ion = _neon(gold)
     bd, banks = ion.bsp, C.Banks(ion.bsp)
     keys, ref = gold["neon_keys"], gold["neon_cell"]
     got = np.array([C.slater_rk_cell(ion.P[a], ion.Q[a], ion.P[b], ion.Q[b], ion.P[c], ion.Q[c], ion.P[d], ion.Q[d],
@@ -73,7 +79,7 @@ def test_scalar_cell_integrals_neon_bitwise(gold):
 
 
 def test_bilinear_and_table_neon(gold):
-    ion = _neon()
+    ion = _neon(gold)
     bd, banks = ion.bsp, C.Banks(ion.bsp)
     M = C.build_slater_rk_bilinear(ion.P[0], ion.Q[0], ion.P[1], ion.Q[1], bd, 1, banks)
     for name, m in zip(("PP", "QQ", "PQ", "QP"), M):
@@ -83,7 +89,7 @@ def test_bilinear_and_table_neon(gold):
 
 
 def test_direct_and_exchange_matrices_neon(gold):
-    ion = _neon()
+    ion = _neon(gold)
     bd, banks = ion.bsp, C.Banks(ion.bsp)
     J = C.direct_potential_cell(ion.P[1], ion.Q[1], bd, 1, banks)
     for name, m in zip(("PP", "QQ"), J):
@@ -95,7 +101,7 @@ def test_direct_and_exchange_matrices_neon(gold):
 
 
 def test_dbsr_fock_blocks_neon(gold):
-    ion = _neon()
+    ion = _neon(gold)
     bd, banks = ion.bsp, C.Banks(ion.bsp)
     n = ion.P.shape[0]
     ad, ax, norms = gold["neon_hf_angular_direct"], gold["neon_hf_angular_exchange"], gold["neon_hf_norms"]
@@ -111,8 +117,7 @@ def test_scalar_cell_integrals_ytterbium(gold):
     """ns = 120: atomx's scalar path is the factored one; the oracle's full
     bank gives the same integrals to ~1e-12 of the largest, and atomx's own
     batched kernel (full bank) agrees with the oracle more closely."""
-    from atomx_b200 import workloads as W
-    ion = W.build_ion(W.ytterbium_scaleup())
+    ion = _Ion(gold, "yb")
     bd, banks = ion.bsp, C.Banks(ion.bsp)
     keys = gold["yb_keys"][:24]
     got = np.array([C.slater_rk_cell(ion.P[a], ion.Q[a], ion.P[b], ion.Q[b], ion.P[c], ion.Q[c], ion.P[d], ion.Q[d],
