@@ -103,3 +103,34 @@ def test_plan_is_cached_read_only_and_ordered():
         o, n = p.k_row_offset[k], p.n_of_k(k)
         assert np.array_equal(p.row_pair[o:o + n], p.pairs_of_k[k]) and np.all(p.row_k[o:o + n] == k)
     assert p.row_pair.shape[0] == sum(p.n_of_k(k) for k in p.ks) == p.n_rows
+
+
+def test_packed_host_tables_expand_symmetric():
+    """HostPackedTables (the host format of slater_rk_tables(host=True,
+    packed=True)): the packed upper triangle of every multipole table expands
+    to the symmetric table, and entry() reads either ordering."""
+    import numpy as np
+    import torch
+
+    from atomx_b200.plan import make_plan
+    from atomx_b200.tables import HostPackedTables, packed_offsets
+    plan = make_plan(np.array([-1, -1, 1, -2, -2, 2]), 3)
+    offs = packed_offsets(plan)
+    rng = np.random.default_rng(3)
+    full = {}
+    vals = np.zeros(plan.unique_entries)
+    for k in plan.ks:
+        n = plan.n_of_k(k)
+        a = rng.normal(size=(n, n))
+        full[k] = a + a.T
+        vals[offs[k]:offs[k] + n * (n + 1) // 2] = full[k][np.triu_indices(n)]
+    last = plan.ks[-1]
+    assert offs[last] + plan.n_of_k(last) * (plan.n_of_k(last) + 1) // 2 == plan.unique_entries
+    t = HostPackedTables(plan=plan, ks=plan.ks, values=torch.from_numpy(vals), offsets=offs, precision="fp64")
+    for k in plan.ks:
+        assert np.array_equal(t.table(k), full[k])
+    k = plan.ks[1]
+    pr = plan.pairs[plan.pairs_of_k[k]]
+    i, j = 0, len(pr) - 1
+    assert t.entry(k, tuple(pr[i]), tuple(pr[j])) == full[k][i, j] == t.entry(k, tuple(pr[j]), tuple(pr[i]))
+    assert t.ordered_entries == plan.ordered_entries and t.unique_entries == plan.unique_entries
