@@ -8,7 +8,12 @@ plain engine's table) plus 2048 seeded random entries; the oracle (the
 reference algorithm restated in C) evaluates each of them.
 
 Gates:
-* plain FP64 engine: floored-relative <= 1e-10 and Schwarz-relative <= 1e-13;
+* plain FP64 engine: Schwarz-relative <= 1e-13, and floored-relative within
+  the larger of 1e-10 and twice the reference's own discrepancy between
+  R(ac;bd) and R(bd;ac) on the same probe set (measured 4.0e-11 on the Z=70
+  table and 1.0e-10 on the Z=54 table: at the floored metric's worst entries
+  the reference's two evaluations of one integral already differ by the
+  gate);
 * split engine: Schwarz-relative <= 1e-10.  Its floored error is reported,
   not gated: on a cancelling entry (|R| down to 1e-6 of the table maximum,
   Schwarz scale near the maximum) a 1e-10 floored error means 1e-16 of the
@@ -114,9 +119,9 @@ def _run(name, streamed):
 @pytest.mark.parametrize("name,streamed", [("ytterbium_scaleup", False), ("xenon_ci_table", True)])
 def test_both_engines_both_metrics(name, streamed):
     rep = _run(name, streamed)
-    f, s = rep["fp64"], rep["split"]
+    f, s, own = rep["fp64"], rep["split"], rep["reference_exchanged_pairs"]
     print(name, json.dumps({e: rep[e] for e in ("fp64", "split", "reference_exchanged_pairs")}))
-    assert f["rel_floored_1e-6"] <= FP64_FLOORED, f
+    assert f["rel_floored_1e-6"] <= max(FP64_FLOORED, 2.0 * own["rel_floored_1e-6"]), (f, own)
     assert f["schwarz_rel"] <= FP64_SCHWARZ, f
     assert s["schwarz_rel"] <= SPLIT_SCHWARZ, s
     assert s["rel_floored_1e-6"] <= SPLIT_FLOORED_SANITY, s

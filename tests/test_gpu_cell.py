@@ -235,7 +235,9 @@ def test_cell_tables_against_batch_and_poisson():
         keys = [(a, c, b, d, k) for a, c in pr for b, d in pr]
         ref = np.array(C.compute_slater_rk_cell_batch(od, keys, ion.bsp)).reshape(T.shape)
         _close(T, ref, 1e-13)
-        assert np.array_equal(T, T.T)
+        # R^k(ac;bd) = R^k(bd;ac): off-diagonal tiles are mirrored, diagonal
+        # tiles compute both orders, which agree to rounding
+        _close(T, T.T, 1e-14)
         _close(T, pois.table(k).cpu().numpy(), 1e-10)
 
 
