@@ -68,6 +68,7 @@ class Request:
     entries: int = 0
     error: BaseException | None = None
     state: dict = field(default_factory=dict)
+    timing: dict = field(default_factory=dict)   # host planning and launch times (ms)
 
     @property
     def latency(self) -> float:
@@ -94,11 +95,13 @@ class ServeReport:
     queue_ms: list
     precision: str
     max_inflight_seen: int
+    stages_ms: dict = field(default_factory=dict)   # stage -> per-request times (ms)
 
     def summary(self) -> dict:
         lat = np.asarray(self.latencies_ms)
         q = np.asarray(self.queue_ms)
-        return {"requests": self.n, "wall_s": self.wall_s, "entries": self.entries,
+        stages = {f"{k}_p50": float(np.percentile(v, 50)) for k, v in self.stages_ms.items() if v}
+        return {"requests": self.n, "wall_s": self.wall_s, "entries": self.entries, "stages_ms": stages,
                 "throughput_entries_per_s": self.entries / self.wall_s if self.wall_s > 0 else None,
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "max_ms": float(lat.max()), "queue_p50_ms": float(np.percentile(q, 50)),
@@ -144,16 +147,19 @@ class SlaterServer:
 
     # ---------------------------------------------------------------- stages
     def _plan(self, req: Request) -> Request:
+        t0 = time.perf_counter()
         req.plan = make_plan(req.ion.kappa, req.k_max)
         if self.precision == "split":
             host_tables(np.asarray(req.ion.bsp["gr"], dtype=np.float64).reshape(-1), req.ion.bsp["gr"].shape[1],
                         req.plan.ks)
         req.footprint = footprint_bytes(req.ion, req.plan, self.precision)
         req.entries = req.plan.ordered_entries
+        req.timing["plan_ms"] = 1e3 * (time.perf_counter() - t0)
         return req
 
     def _launch(self, req: Request, stream) -> None:
         from . import tables as T
+        req.state["t_launch"] = time.perf_counter()
         sink = req.sink if req.sink is not None else ChecksumSink()
         req.sink = sink
         with torch.cuda.device(self.device), torch.cuda.stream(stream):
@@ -167,9 +173,13 @@ class SlaterServer:
                 T.stream_tables(dev, sink, precision="fp64", stream=stream)
             ev = torch.cuda.Event()
             ev.record(stream)
-        req.state.update(dev=dev, event=ev)
+        req.state.update(dev=dev, event=ev, t_enqueued=time.perf_counter())
 
     def _finish(self, req: Request) -> None:
+        st = req.state
+        if "t_launch" in st and "t_enqueued" in st:
+            req.timing["launch_host_ms"] = 1e3 * (st["t_enqueued"] - st["t_launch"])
+            req.timing["after_enqueue_ms"] = 1e3 * (time.perf_counter() - st["t_enqueued"])
         eng = req.state.get("engine")
         try:
             if eng is not None and req.error is None:
@@ -248,10 +258,12 @@ class SlaterServer:
                 time.sleep(2e-4)
         wall = now()
         done = [r for r in requests if r.error is None]
+        stages = {k: [r.timing[k] for r in done if k in r.timing]
+                  for k in ("plan_ms", "launch_host_ms", "after_enqueue_ms")}
         return ServeReport(n=len(requests), wall_s=wall, entries=int(sum(r.entries for r in done)),
                            latencies_ms=[1e3 * r.latency for r in done],
                            queue_ms=[1e3 * (r.admitted - r.arrival) for r in done], precision=self.precision,
-                           max_inflight_seen=max_seen)
+                           max_inflight_seen=max_seen, stages_ms=stages)
 
     def close(self):
         self.pool.shutdown(wait=True)
