@@ -16,9 +16,9 @@ ordered entries = sum_k n_k^2, unique entries = sum_k n_k (n_k + 1) / 2.
 """
 from __future__ import annotations
 
-from dataclasses import dataclass
-
 import threading
+from dataclasses import dataclass
+from functools import lru_cache
 
 import numpy as np
 
@@ -94,6 +94,27 @@ def make_plan(kappa, k_max: int) -> TablePlan:
     return plan
 
 
+@lru_cache(maxsize=4096)
+def _allowed_mask(kappa_a: int, kappa_c: int, k_max: int) -> tuple:
+    """k <= k_max allowed for a pair of these kappas, as a tuple of bools."""
+    al = set(exchange_k_range(kappa_a, kappa_c))
+    return tuple(k in al for k in range(k_max + 1))
+
+
+def _triu_rows(l: np.ndarray, n: np.ndarray):
+    """(row, col) of position l in the a-major upper triangle (diagonal
+    included) of an n x n block: row i starts at i n - i (i - 1) / 2."""
+    b = 2 * n + 1
+    i = np.floor((b - np.sqrt(b.astype(np.float64) ** 2 - 8.0 * l)) / 2.0).astype(np.int64)
+    for _ in range(2):  # guard the square root's rounding
+        start = i * n - i * (i - 1) // 2
+        i = np.where(start > l, i - 1, i)
+        nxt = (i + 1) * n - (i + 1) * i // 2
+        i = np.where(nxt <= l, i + 1, i)
+    start = i * n - i * (i - 1) // 2
+    return i, i + (l - start)
+
+
 def _make_plan(kappa, k_max: int) -> TablePlan:
     n = kappa.shape[0]
     if n == 0:
@@ -101,31 +122,31 @@ def _make_plan(kappa, k_max: int) -> TablePlan:
     if k_max < 0:
         raise ValueError("k_max must be a nonnegative integer")
     # Shells: maximal runs of equal kappa in orbital order.
-    starts = [0] + [i for i in range(1, n) if kappa[i] != kappa[i - 1]]
-    shells = [(int(kappa[s]), s, (starts[j + 1] if j + 1 < len(starts) else n)) for j, s in enumerate(starts)]
-    pair_parts, block_parts, blocks, allowed_of_block = [], [], [], []
-    count = 0
-    for i, (ka, sa, ea) in enumerate(shells):
-        for j in range(i, len(shells)):
-            kc, sc, ec = shells[j]
-            if i == j:  # a <= c within the shell, a-major order
-                a, c = np.triu_indices(ea - sa)
-                a, c = a + sa, c + sa
-            else:
-                a = np.repeat(np.arange(sa, ea), ec - sc)
-                c = np.tile(np.arange(sc, ec), ea - sa)
-            pair_parts.append(np.stack([a, c], axis=1))
-            block_parts.append(np.full(a.shape[0], len(blocks), dtype=np.int64))
-            blocks.append((ka, kc, count, count + a.shape[0]))
-            count += a.shape[0]
-            allowed_of_block.append([k for k in exchange_k_range(ka, kc) if k <= k_max])
-    pairs = np.concatenate(pair_parts).astype(np.int64).reshape(-1, 2)
-    pblock = np.concatenate(block_parts)
-    ks = sorted({k for al in allowed_of_block for k in al})
-    pairs_of_k = {}
-    for k in ks:
-        idx = [np.arange(b[2], b[3]) for bi, b in enumerate(blocks) if k in allowed_of_block[bi]]
-        pairs_of_k[k] = np.concatenate(idx).astype(np.int64) if idx else np.zeros(0, np.int64)
+    cut = np.flatnonzero(kappa[1:] != kappa[:-1]) + 1
+    starts = np.concatenate([[0], cut]).astype(np.int64)
+    sizes = np.diff(np.concatenate([starts, [n]])).astype(np.int64)
+    skap = kappa[starts]
+    # Blocks: shell pairs (i <= j) in i-major order; pairs a <= c within a shell, a-major.
+    si, sj = np.triu_indices(starts.shape[0])
+    same = si == sj
+    na, nc = sizes[si], sizes[sj]
+    bsize = np.where(same, na * (na + 1) // 2, na * nc)
+    boff = np.concatenate([[0], np.cumsum(bsize)]).astype(np.int64)
+    total = int(boff[-1])
+    bid = np.repeat(np.arange(si.shape[0]), bsize)
+    loc = np.arange(total, dtype=np.int64) - boff[bid]
+    ncb = nc[bid]
+    a_loc, c_loc = loc // ncb, loc % ncb
+    sm = same[bid]
+    if sm.any():
+        a_loc[sm], c_loc[sm] = _triu_rows(loc[sm], na[bid][sm])
+    pairs = np.stack([starts[si][bid] + a_loc, starts[sj][bid] + c_loc], axis=1).astype(np.int64)
+    pblock = bid.astype(np.int64)
+    allowed = np.array([_allowed_mask(int(skap[a]), int(skap[b]), int(k_max)) for a, b in zip(si, sj)],
+                       dtype=bool).reshape(si.shape[0], k_max + 1)
+    blocks = [(int(skap[a]), int(skap[b]), int(boff[t]), int(boff[t + 1])) for t, (a, b) in enumerate(zip(si, sj))]
+    ks = [int(k) for k in np.flatnonzero(allowed.any(axis=0))]
+    pairs_of_k = {k: np.flatnonzero(allowed[pblock, k]).astype(np.int64) for k in ks}
     off, pos = {}, 0
     for k in ks:
         off[k] = pos
