@@ -76,7 +76,11 @@ class Request:
 
 
 class ChecksumSink:
-    """Consumes every table on the device: per-(k, kappa-block) sums."""
+    """Consumes every table on the device: per-(k, kappa-block) sums.  It
+    keeps one result per multipole, so a later delivery of the same k (a
+    table recomputed after a failed certificate) replaces the earlier one."""
+
+    replaces_tables = True
 
     def __init__(self):
         self.sums = {}

@@ -466,17 +466,31 @@ class SplitEngine:
         (see ``tables.stream_tables``); the whole table is never held.  The
         call waits once, after the row kernels, for the per-table certificate
         (tables that fail it are recomputed in FP64 before they reach the
-        sink).  With ``check=False`` nothing else waits for the device: call
-        ``check_status()`` once the stream's work is known to be done, to
-        raise a contraction error."""
+        sink).  A sink with ``replaces_tables = True`` (one table per
+        multipole, a later delivery of the same k replacing the earlier) is
+        served without that wait: every table is contracted at once and
+        ``check_status()`` recomputes a table whose certificate failed in FP64
+        and delivers it again.  With ``check=False`` nothing else waits for the
+        device: call ``check_status()`` once the stream's work is known to be
+        done, to raise a contraction error."""
         s = stream if stream is not None else torch.cuda.current_stream()
         plan = self.dev.plan
         self.rows(s)
-        # which tables go to FP64 is known from the rows alone: one wait here,
-        # on this stream only and without holding the GIL (serving launches
-        # requests from several host threads)
-        _, (_, flagged) = read_status(self.status, s)
-        fp64 = set(self._failing(self.est.cpu().numpy())) if flagged else set()
+        self._sink = sink
+        if getattr(sink, "replaces_tables", False):
+            # the sink keeps one table per multipole and takes a later
+            # delivery of the same k in its place: every table is contracted
+            # at once, without waiting for the certificate, and check_status()
+            # recomputes a failing table in FP64 and delivers it again
+            fp64 = set()
+            self._deferred = True
+        else:
+            # which tables go to FP64 is known from the rows alone: one wait
+            # here, on this stream only and without holding the GIL (serving
+            # launches requests from several host threads)
+            _, (_, flagged) = read_status(self.status, s)
+            fp64 = set(self._failing(self.est.cpu().numpy())) if flagged else set()
+            self._deferred = False
         self.escalated = sorted(fp64)
         nmax = max(plan.n_of_k(k) for k in plan.ks)
         bufs = [torch.empty(nmax * nmax, dtype=torch.float64, device=self.resA.device) for _ in range(2)]
@@ -572,6 +586,17 @@ class SplitEngine:
             _native.check(st, "crt_syrk_kernel")
         if getattr(self, "_streamed", False):  # the stream path chose per table already
             self._streamed = False
+            if getattr(self, "_deferred", False):
+                self._deferred = False
+                self.escalated = self._failing(self.est.cpu().numpy()) if flagged else []
+                plan = self.dev.plan
+                for k in self.escalated:  # recompute in FP64 and deliver again
+                    nk = plan.n_of_k(k)
+                    buf = torch.empty(nk * nk, dtype=torch.float64, device=self.resA.device)
+                    self._recompute(((k, 0),)).run(buf, s)
+                    self._sink(k, buf.view(nk, nk), plan.block_ranges_of_k(k), s)
+                if self.escalated:
+                    s.synchronize()
             return
         self.escalated = []
         if flagged and self.out is not None:

@@ -418,8 +418,11 @@ def iter_blocks(table: torch.Tensor, blocks):
 class HostTableSink:
     """Sink that copies each multipole table to pinned host memory.
 
-    ``tables[k]`` is valid after ``wait()`` (or ``wait(k)``).
+    ``tables[k]`` is valid after ``wait()`` (or ``wait(k)``).  One table is
+    kept per multipole: a later delivery of the same k replaces it.
     """
+
+    replaces_tables = True
 
     def __init__(self):
         self.tables, self._events = {}, {}

@@ -180,3 +180,34 @@ def test_uneven_batch_of_64_ions_within_gate():
     groups = len(b.group_of)
     assert 1 <= len(b.escalated) <= groups // 10, b.escalated
     assert (CANCELLING_ION, CANCELLING_K) in b.escalated
+
+
+def test_deferred_certificate_redelivers_the_fp64_table(cancelling):
+    """A sink that keeps one table per multipole (replaces_tables) is served
+    without the mid-stream wait for the certificate: every table is
+    contracted at once and check_status() hands the failing table to the
+    sink again, recomputed in FP64.  Its final tables equal those of a sink
+    served the strict way (the certificate read before any contraction)."""
+    from atomx_b200.split import SplitEngine
+
+    class Keep:
+        def __init__(self, replaces):
+            self.replaces_tables = replaces
+            self.tables, self.calls = {}, []
+
+        def __call__(self, k, table, blocks, stream):
+            with torch.cuda.stream(stream):
+                self.tables[k] = table.clone()
+            self.calls.append(k)
+
+    ion, Pg, Qg, dev = cancelling
+    strict, lazy = Keep(False), Keep(True)
+    SplitEngine(dev, materialize=False).stream_tables(strict, check=True)
+    eng = SplitEngine(dev, materialize=False)
+    eng.stream_tables(lazy, check=True)
+    torch.cuda.synchronize()
+    assert CANCELLING_K in eng.escalated
+    assert strict.calls == list(dev.plan.ks)
+    assert lazy.calls == list(dev.plan.ks) + list(eng.escalated)
+    for k in dev.plan.ks:
+        assert torch.equal(strict.tables[k], lazy.tables[k]), k
