@@ -48,8 +48,9 @@ __all__ = ["Request", "ServeReport", "SlaterServer", "ChecksumSink", "footprint_
 
 #: The latency bound the loop is held to on the mixed-ion stream (Poisson
 #: arrivals at 200 requests/s, Z 2..92, 30..200 B-splines, 10..300 spinors,
-#: k_max 2..14): the 99th percentile of (last table delivered - arrival).
-P99_BOUND_MS = 1000.0
+#: k_max 2..14): the 99th percentile of (last table delivered - arrival),
+#: with two requests on the GPU at once.
+P99_BOUND_MS = 500.0
 
 
 @dataclass

@@ -574,7 +574,7 @@ def serve_leg(args) -> dict:
         warm.serve([Request(rid=-1, ion=ions[0], k_max=stream[0][1].k_max)], realtime=False)
         warm.close()
         torch_sync()
-        server = SlaterServer(precision=precision, max_inflight=args.serve_slots, workers=8)
+        server = SlaterServer(precision=precision, max_inflight=args.serve_slots, workers=4)
         rep = server.serve(reqs, realtime=True)
         server.close()
         torch_sync()
@@ -908,7 +908,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
     ap.add_argument("--serve", type=int, default=300, help="requests in the serving leg (0 = skip)")
-    ap.add_argument("--serve-slots", type=int, default=8, help="requests on the GPU at once in the serving leg")
+    ap.add_argument("--serve-slots", type=int, default=2, help="requests on the GPU at once in the serving leg")
     ap.add_argument("--no-grid", action="store_true", help="skip the arbitrary-grid Y^k leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-ion batch leg")
     ap.add_argument("--no-stream", action="store_true", help="skip the streamed Z=54 CI table leg")
