@@ -19,8 +19,12 @@
 // eigenproblems here are solved by cyclic Jacobi rotations (ng <= 32), so
 // eigenvector signs may differ, which leaves every z_e z_e^T and the factor
 // unchanged.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "rkb_common.cuh"
@@ -192,4 +196,73 @@ extern "C" long rkb_green_factor(const double *r, int nv, int ng, int k, double 
         for (int i = 0; i < ng; ++i) *o++ = zvec[(size_t)e * ng + i];
     }
     return total;
+}
+
+// All multipoles' factor tables of one grid in one call: the factorisations
+// (each the serial recursion of rkb_green_factor) run on up to nthreads host
+// threads, one multipole per task, then the packed tables are laid end to end
+// in ks order and the cell-minor copy is written beside them.  A serving
+// planner gets every table of a request without the interpreter lock and
+// without a transpose pass of its own.
+extern "C" long rkb_green_tables(const double *r, int nv, int ng, const int *ks, int nk, double tau,
+                                 const double *mo, const double *mi, int nthreads, int kmax, double *flat,
+                                 long flat_cap, long *koff, double *flat_t, long flat_t_cap, long *koff_t,
+                                 long *nz) {
+    RKB_CHECK_ARG(r != nullptr && ks != nullptr && mo != nullptr && mi != nullptr && flat != nullptr &&
+                      koff != nullptr && flat_t != nullptr && koff_t != nullptr && nz != nullptr,
+                  "null argument");
+    RKB_CHECK_ARG(nk >= 1 && nv >= 2 && ng >= 1 && ng <= RKB_MAX_NG, "invalid grid or multipole count");
+    for (int i = 0; i < nk; ++i)
+        RKB_CHECK_ARG(ks[i] >= 0 && ks[i] <= kmax && (i == 0 || ks[i] > ks[i - 1]),
+                      "multipoles must be increasing and within 0..kmax (%d)", kmax);
+    const int n = nv * ng, g2 = ng * ng;
+    const long cap1 = (long)n + (long)nv * g2 + (long)n + ng + g2 + 2 + (long)n * (ng + 1);
+    const long per_t = 2L * n + (long)nv * g2;
+    std::vector<std::vector<double>> tab((size_t)nk);
+    std::vector<long> got((size_t)nk, 0);
+    std::vector<std::string> err((size_t)nk);
+    std::atomic<int> next(0);
+    auto work = [&]() {
+        for (int i = next.fetch_add(1); i < nk; i = next.fetch_add(1)) {
+            tab[(size_t)i].resize((size_t)cap1);
+            got[(size_t)i] = rkb_green_factor(r, nv, ng, ks[i], tau, mo, mi, tab[(size_t)i].data(), cap1);
+            if (got[(size_t)i] < 0) err[(size_t)i] = rkb_last_error();
+        }
+    };
+    const int nt = std::max(1, std::min(nthreads, nk));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+    for (int i = 0; i < nk; ++i)
+        if (got[(size_t)i] < 0) {
+            set_error("%s", err[(size_t)i].c_str());
+            return got[(size_t)i];
+        }
+    for (int k = 0; k <= kmax; ++k) koff[k] = koff_t[k] = -1;
+    long pos = 0, pos_t = 0;
+    for (int i = 0; i < nk; ++i) {
+        const long len = got[(size_t)i];
+        RKB_CHECK_ARG(pos + len <= flat_cap && pos_t + per_t <= flat_t_cap, "table capacity too small");
+        const double *F = tab[(size_t)i].data();
+        std::memcpy(flat + pos, F, sizeof(double) * (size_t)len);
+        koff[ks[i]] = pos;
+        nz[i] = (long)F[(long)n + (long)nv * g2 + n + ng + g2 + 1];
+        // cell-minor copy: u^T[ng][nv] | C^T[ng][nv] | Lb as [ng][ng][nv]
+        double *T = flat_t + pos_t;
+        const double *u = F, *Lb = F + n, *C = F + n + (long)nv * g2;
+        for (int m = 0; m < nv; ++m)
+            for (int j = 0; j < ng; ++j) {
+                T[(long)j * nv + m] = u[(long)m * ng + j];
+                T[(long)n + (long)j * nv + m] = C[(long)m * ng + j];
+            }
+        for (int m = 0; m < nv; ++m)
+            for (int a = 0; a < ng; ++a)
+                for (int b = 0; b < ng; ++b)
+                    T[2L * n + ((long)a * ng + b) * nv + m] = Lb[(long)m * g2 + (long)a * ng + b];
+        koff_t[ks[i]] = pos_t;
+        pos += len;
+        pos_t += per_t;
+    }
+    return pos;
 }

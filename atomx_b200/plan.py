@@ -59,13 +59,20 @@ class TablePlan:
         return int(sum(self.n_of_k(k) * (self.n_of_k(k) + 1) // 2 for k in self.ks))
 
     def block_ranges_of_k(self, k: int):
-        """[(block_id, start, stop)] row ranges of the k-th table."""
-        bid = self.pair_block[self.pairs_of_k[k]]
-        if bid.shape[0] == 0:
-            return []
-        starts = np.concatenate([[0], np.flatnonzero(bid[1:] != bid[:-1]) + 1])
-        stops = np.concatenate([starts[1:], [bid.shape[0]]])
-        return [(int(bid[a]), int(a), int(b)) for a, b in zip(starts, stops)]
+        """[(block_id, start, stop)] row ranges of the k-th table (computed
+        once per plan and k; a fresh list each call)."""
+        cache = self.__dict__.setdefault("_block_ranges", {})
+        hit = cache.get(k)
+        if hit is None:
+            bid = self.pair_block[self.pairs_of_k[k]]
+            if bid.shape[0] == 0:
+                hit = ()
+            else:
+                starts = np.concatenate([[0], np.flatnonzero(bid[1:] != bid[:-1]) + 1])
+                stops = np.concatenate([starts[1:], [bid.shape[0]]])
+                hit = tuple((int(bid[a]), int(a), int(b)) for a, b in zip(starts, stops))
+            cache[k] = hit
+        return list(hit)
 
 
 _plan_cache: dict = {}

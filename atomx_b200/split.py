@@ -29,6 +29,7 @@ from . import _native
 from .split_plan import (bits_for_moduli, concat_tables, crt_constants, green_factor_packed, moduli_needed,
                          table_z_count)
 from .tables import Fp64Recompute, IonDevice, tile_tasks
+from .yk import yk_partial_matrices
 
 __all__ = ["SplitEngine", "IonRows", "factors_for_grid", "host_tables", "choose_width", "DEFAULT_BITS"]
 
@@ -86,13 +87,19 @@ def check_kdim(kdim: int) -> None:
 
 def choose_width(bits, n_mod, kdim: int) -> tuple[int, int]:
     """(bits, n_mod) for a contraction length: explicit values are kept;
-    bits=None takes the fewest moduli for DEFAULT_BITS and the widest split
-    those moduli hold."""
-    if bits is not None:
-        bits = int(bits)
-        return bits, (int(n_mod) if n_mod is not None else moduli_needed(bits, kdim))
-    n_mod = int(n_mod) if n_mod is not None else moduli_needed(DEFAULT_BITS, kdim)
-    return max(DEFAULT_BITS, bits_for_moduli(n_mod, kdim)), n_mod
+    bits=None takes the widest split the moduli hold, and n_mod=None the
+    fewest moduli for ``bits`` (DEFAULT_BITS when bits is None too).  Raises
+    when the moduli cannot hold the products of the split exactly."""
+    if n_mod is None:
+        n_mod = moduli_needed(DEFAULT_BITS if bits is None else int(bits), kdim)
+    n_mod = int(n_mod)
+    held = bits_for_moduli(n_mod, kdim)
+    bits = held if bits is None else int(bits)
+    if bits > held:
+        raise ValueError(f"{n_mod} moduli hold {held}-bit splits of length {kdim}, not {bits}")
+    return bits, n_mod
+
+
 _factor_cache: dict = {}
 _factor_lock = threading.Lock()
 
@@ -118,6 +125,10 @@ def factors_for_grid(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict
 
 
 _host_cache: dict = {}
+#: host threads one host_tables call factorises its multipoles on (one: the
+#: work is about 0.1 ms per multipole, and a serving planner pool already
+#: runs requests side by side)
+HOST_TABLE_THREADS = 1
 
 
 def host_tables(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
@@ -132,26 +143,33 @@ def host_tables(r_flat: np.ndarray, ng: int, ks, tau: float = 1e-3) -> dict:
         hit = _host_cache.get(key)
     if hit is not None:
         return hit
-    factors = factors_for_grid(r_flat, ng, ks, tau=tau)
     nv = r_flat.shape[0] // ng
     n = nv * ng
     kmax = max(ks)
-    flat, offs = concat_tables([factors[k] for k in ks])
-    koff = np.full(kmax + 1, -1, dtype=np.int64)
-    koff_t = np.full(kmax + 1, -1, dtype=np.int64)
-    parts, pos = [], 0
-    for i, k in enumerate(ks):
-        koff[k] = offs[i]
-        F = factors[k]
-        u_ = F[:n].reshape(nv, ng).T
-        L_ = F[n:n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
-        C_ = F[n + nv * ng * ng:n + nv * ng * ng + n].reshape(nv, ng).T
-        t = np.concatenate([u_.ravel(), C_.ravel(), L_.ravel()])
-        koff_t[k] = pos
-        pos += t.shape[0]
-        parts.append(t)
-    out = {"factors": factors, "flat": flat, "koff": koff, "flat_t": np.concatenate(parts), "koff_t": koff_t,
-           "nz": {k: table_z_count(factors[k], nv, ng) for k in ks}}
+    mo, mi = yk_partial_matrices(ng)
+    mo = np.ascontiguousarray(mo, dtype=np.float64)
+    mi = np.ascontiguousarray(mi, dtype=np.float64)
+    kk = np.asarray(ks, dtype=np.int32)
+    cap1 = n + nv * ng * ng + n + ng + ng * ng + 2 + n * (ng + 1)
+    flat = np.empty(len(ks) * cap1, dtype=np.float64)
+    flat_t = np.empty(len(ks) * (2 * n + nv * ng * ng), dtype=np.float64)
+    koff = np.empty(kmax + 1, dtype=np.int64)
+    koff_t = np.empty(kmax + 1, dtype=np.int64)
+    nz = np.empty(len(ks), dtype=np.int64)
+    L = _native.load()
+    # one native call (ctypes drops the interpreter lock for it): every
+    # multipole factorised, the tables laid end to end, the cell-minor copy
+    got = L.rkb_green_tables(r_flat.ctypes.data, nv, ng, kk.ctypes.data, len(ks), float(tau), mo.ctypes.data,
+                             mi.ctypes.data, HOST_TABLE_THREADS, kmax, flat.ctypes.data, flat.shape[0],
+                             koff.ctypes.data, flat_t.ctypes.data, flat_t.shape[0], koff_t.ctypes.data,
+                             nz.ctypes.data)
+    if got < 0:
+        _native.check(int(-got), "rkb_green_tables")
+    flat = flat[:got].copy()
+    ends = [int(koff[k]) for k in ks[1:]] + [int(got)]
+    factors = {k: flat[int(koff[k]):e] for k, e in zip(ks, ends)}
+    out = {"factors": factors, "flat": flat, "koff": koff, "flat_t": flat_t, "koff_t": koff_t,
+           "nz": {k: int(z) for k, z in zip(ks, nz)}}
     with _factor_lock:
         if len(_host_cache) > 256:
             _host_cache.clear()

@@ -122,15 +122,17 @@ def upload_values(Pv, Qv, kappa, gr, grw, k_max: int, plan: TablePlan | None = N
 
 
 def tile_tasks(sizes, tile: int = TILE):
-    """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes."""
-    parts = []
-    for g, n in enumerate(sizes):
-        nt = (int(n) + tile - 1) // tile
-        ti, tj = np.triu_indices(nt)
-        parts.append(np.stack([np.full(ti.shape[0], g), ti, tj], axis=1))
-    if not parts:
+    """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes
+    (each group's tiles row-major, groups in order)."""
+    nt = (np.asarray(sizes, dtype=np.int64).reshape(-1) + tile - 1) // tile
+    if nt.shape[0] == 0 or not nt.any():
         return np.zeros((0, 3), dtype=np.int32)
-    return np.concatenate(parts).astype(np.int32).reshape(-1, 3)
+    # row-major upper triangle of the largest group; a group of nt tiles per
+    # side takes the entries with tj < nt, in the same order
+    ti, tj = np.triu_indices(int(nt.max()))
+    keep = tj[None, :] < nt[:, None]                      # (groups, triangle)
+    g, e = np.nonzero(keep)
+    return np.stack([g, ti[e], tj[e]], axis=1).astype(np.int32)
 
 
 @dataclass

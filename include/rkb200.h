@@ -295,6 +295,19 @@ int rkb_split_rows_cells(const double *d_Pv, const double *d_Qv, long orb_ld, co
 long rkb_green_factor(const double *r, int nv, int ng, int k, double tau, const double *mo,
                       const double *mi, double *out, long cap);
 
+/* Host-only planning: the factor tables of every multipole ks[0..nk)
+ * (increasing, <= kmax) on one grid, each as rkb_green_factor writes it,
+ * computed on up to nthreads host threads.  flat gets the tables end to end
+ * in ks order (koff[k] = start, -1 for k <= kmax not in ks; at most flat_cap
+ * doubles), nz[i] the Z-column count of ks[i], and flat_t the cell-minor copy
+ * the cell row kernel reads (rkb_split_rows_cells d_ktab_t): per multipole
+ * u^T[ng][nv] | C^T[ng][nv] | Lb as [ng][ng][nv] at koff_t[k] (2N + nv ng^2
+ * doubles each; at most flat_t_cap).  Returns the doubles written to flat
+ * or a negative rkb_status.  No atomx counterpart (see rkb_green_factor). */
+long rkb_green_tables(const double *r, int nv, int ng, const int *ks, int nk, double tau, const double *mo,
+                      const double *mi, int nthreads, int kmax, double *flat, long flat_cap, long *koff,
+                      double *flat_t, long flat_t_cap, long *koff_t, long *nz);
+
 /* Residue positions spanned by the body in rkb_split_rows_fused's layout (a
  * multiple of 128), or -1 for an invalid grid.  Host-only, no device work. */
 long rkb_split_fused_body_width(int nv, int ng);

@@ -20,6 +20,20 @@ def test_batch_tasks_cover_upper_tiles_and_lpt_orders_by_cost():
         batch_tasks(sizes, costs, "random")
 
 
+def test_tile_tasks_are_each_groups_upper_triangle_in_order():
+    from atomx_b200.tables import tile_tasks
+    rng = np.random.default_rng(0)
+    for trial in range(60):
+        sizes = rng.integers(0, 3000, rng.integers(0, 30)) if trial % 7 else np.zeros(trial % 3, int)
+        ref = []
+        for g, n in enumerate(sizes):
+            ti, tj = np.triu_indices((int(n) + 127) // 128)
+            ref += [(g, a, b) for a, b in zip(ti, tj)]
+        got = tile_tasks(sizes)
+        assert got.dtype == np.int32 and got.shape == (len(ref), 3)
+        assert [tuple(map(int, t)) for t in got] == ref
+
+
 def test_split_width_choice():
     from atomx_b200.split import KDIM_MAX, check_kdim, choose_width
     from atomx_b200.split_plan import MODULI, bits_for_moduli, moduli_needed
@@ -31,6 +45,10 @@ def test_split_width_choice():
         assert 2 * kdim * (1 << (2 * bits)) + 2 < math.prod(MODULI[:n_mod])
         assert bits == max(36, bits_for_moduli(n_mod, kdim))
     assert choose_width(30, None, 896) == (30, moduli_needed(30, 896))
+    # fixed moduli: the widest split they hold at each length, and no wider
+    assert choose_width(None, 11, 256) == (39, 11) and choose_width(None, 11, KDIM_MAX) == (37, 11)
+    with pytest.raises(ValueError):
+        choose_width(38, 10, 1024)
     with pytest.raises(ValueError):
         check_kdim(KDIM_MAX + 128)
 
@@ -66,6 +84,43 @@ def test_cell_minor_tables_are_transposes_of_the_packed_ones():
         np.testing.assert_array_equal(T[n:2 * n].reshape(ng, nv), C.T)
         np.testing.assert_array_equal(T[2 * n:2 * n + nv * ng * ng].reshape(ng, ng, nv), L.transpose(1, 2, 0))
     assert host_tables(gr.ravel(), ng, [0, 1, 2]) is H  # cached
+
+
+@pytest.mark.parametrize("name,ks", [("neon_small", (0, 1, 2)), ("ytterbium_scaleup", tuple(range(13))),
+                                     ("neon_small", (1, 3, 4))])
+@pytest.mark.parametrize("threads", [1, 3])
+def test_host_tables_equal_the_per_multipole_factors(name, ks, threads, monkeypatch):
+    """host_tables (one native call over all multipoles) equals the
+    per-multipole factorisation laid end to end, with the cell-minor copy
+    built by transposes, bit for bit, on one host thread or several."""
+    from atomx_b200 import split as SP
+    from atomx_b200 import workloads as W
+    monkeypatch.setattr(SP, "HOST_TABLE_THREADS", threads)
+    ion = W.build_ion(getattr(W, name)())
+    gr = np.asarray(ion.bsp["gr"], dtype=np.float64)
+    nv, ng = gr.shape
+    n = nv * ng
+    SP._host_cache.clear()
+    H = SP.host_tables(gr.ravel(), ng, ks)
+    F = SP.factors_for_grid(gr.ravel(), ng, ks)
+    assert np.array_equal(H["flat"], np.concatenate([F[k] for k in ks]))
+    pos = pos_t = 0
+    for k in range(max(ks) + 1):
+        if k not in ks:
+            assert H["koff"][k] == -1 and H["koff_t"][k] == -1
+            continue
+        assert H["koff"][k] == pos and np.array_equal(H["factors"][k], F[k])
+        Fk = F[k]
+        u_ = Fk[:n].reshape(nv, ng).T
+        L_ = Fk[n:n + nv * ng * ng].reshape(nv, ng, ng).transpose(1, 2, 0)
+        C_ = Fk[n + nv * ng * ng:n + nv * ng * ng + n].reshape(nv, ng).T
+        t = np.concatenate([u_.ravel(), C_.ravel(), L_.ravel()])
+        assert H["koff_t"][k] == pos_t and np.array_equal(H["flat_t"][pos_t:pos_t + t.shape[0]], t)
+        assert H["nz"][k] == int(Fk[n + nv * ng * ng + n + ng + ng * ng + 1])
+        pos += Fk.shape[0]
+        pos_t += t.shape[0]
+    assert H["flat_t"].shape[0] == pos_t
+    SP._host_cache.clear()
 
 
 def test_serving_footprint_grows_with_the_request():
