@@ -88,16 +88,28 @@ class SplitBatch(_Graphable):
 
     def __init__(self, devs: list[IonDevice], bits: int | None = None, tau: float = 1e-3, fused=None,
                  corr_floor: float | None = None, order: str = "lpt", n_mod: int | None = None,
-                 cert_limit: float = CERT_LIMIT):
+                 cert_limit: float = CERT_LIMIT, ion_widths: bool = False, ion_rows: list | None = None):
         _native.require_device()
         if not devs:
             raise ValueError("empty batch")
         self.devs, self.order = list(devs), order
-        self.ions = [IonRows(d, tau=tau, fused=fused) for d in self.devs]
+        if ion_rows is not None:  # row sides built ahead (e.g. by a serving planner)
+            if len(ion_rows) != len(self.devs) or any(r.dev is not d for r, d in zip(ion_rows, self.devs)):
+                raise ValueError("ion_rows must be the IonRows of devs, in order")
+            self.ions = list(ion_rows)
+        else:
+            self.ions = [IonRows(d, tau=tau, fused=fused) for d in self.devs]
         d = self.devs[0].Pv.device
         self.kpad = max(r.kmax_dim for r in self.ions)
         check_kdim(self.kpad)
         self.bits, self.n_mod = choose_width(bits, n_mod, self.kpad)
+        #: split width of each ion's rows.  With ``ion_widths`` every ion takes
+        #: the widest split the batch's moduli hold at its own contraction
+        #: length (or ``bits``), so an ion's rows, and with a fixed n_mod and
+        #: corr_floor its tables, do not depend on the other ions of the batch.
+        self.ion_bits = [choose_width(bits, self.n_mod, r.kmax_dim)[0] if ion_widths else self.bits
+                         for r in self.ions]
+        self.bits = min(self.ion_bits)
         self.moduli, self.f_hi, self.f_lo, self.M, self.pair_inv = crt_constants(self.n_mod)
         self.cw = max(dv.ng for dv in self.devs) + 2  # g_0 and the two coupling moments
         self.cwp = _round_up(self.cw, 2)
@@ -125,13 +137,16 @@ class SplitBatch(_Graphable):
         offs = np.concatenate([[0], np.cumsum(np.asarray(g_n, dtype=np.int64) ** 2)])
         self.offsets = {gk: int(offs[j]) for j, gk in enumerate(self.group_of)}
         self.total = int(offs[-1])
-        self.grp_row0 = torch.as_tensor(g_row0, dtype=torch.int64, device=d)
-        self.grp_n = torch.as_tensor(g_n, dtype=torch.int64, device=d)
-        self.grp_kdim = torch.as_tensor(g_kdim, dtype=torch.int64, device=d)
-        self.grp_out = torch.as_tensor(offs[:-1], dtype=torch.int64, device=d)
         tasks = batch_tasks(g_n, g_kdim, order)
         self.n_tasks = int(tasks.shape[0])
-        self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
+        # the group records and the task list in one host-to-device copy
+        ng_ = len(g_n)
+        host = np.empty(4 * ng_ + (tasks.size + 1) // 2, dtype=np.int64)
+        host[:4 * ng_] = np.concatenate([g_row0, g_n, g_kdim, offs[:-1]]).astype(np.int64)
+        host[4 * ng_:].view(np.int32)[:tasks.size] = tasks.reshape(-1)
+        arr = torch.from_numpy(host).to(d)
+        self.grp_row0, self.grp_n, self.grp_kdim, self.grp_out = (arr[i * ng_:(i + 1) * ng_] for i in range(4))
+        self.tasks = arr[4 * ng_:].view(torch.int32)[:tasks.size]
         #: [contraction status, number of tables whose certificate failed]
         self.status = torch.zeros(2, dtype=torch.int32, device=d)
         self.est = torch.zeros(len(g_n), dtype=torch.float64, device=d)
@@ -157,15 +172,18 @@ class SplitBatch(_Graphable):
     #: side streams the per-ion row launches are spread over
     ROW_STREAMS = 4
 
-    def rows(self, stream=None) -> None:
+    def rows(self, stream=None, side_streams=None) -> None:
         """Every ion's row kernels, then the certificate.  Ions on the cell or
-        fused kernel go round-robin to ROW_STREAMS side streams forked from and
-        joined back to ``stream`` (a fork/join that graph capture records), so
-        small ions fill the GPU side by side; two-kernel ions share the FP64
-        workspace and stay in order on ``stream``."""
+        fused kernel go round-robin to side streams (``side_streams``, else
+        ROW_STREAMS of the batch's own) forked from and joined back to
+        ``stream`` (a fork/join that graph capture records), so small ions
+        fill the GPU side by side; two-kernel ions share the FP64 workspace
+        and stay in order on ``stream``."""
         s = stream if stream is not None else torch.cuda.current_stream()
         self._stream = stream
-        if not hasattr(self, "_side"):
+        if side_streams is not None:
+            self._side = list(side_streams)
+        elif not hasattr(self, "_side"):
             self._side = [torch.cuda.Stream(device=s.device) for _ in range(self.ROW_STREAMS)]
         fork = torch.cuda.Event()
         fork.record(s)
@@ -180,7 +198,7 @@ class SplitBatch(_Graphable):
                 if ls not in used:
                     ls.wait_event(fork)
                     used.add(ls)
-            r.launch(self.bits, self.n_mod, self._c[0], self.resA, self.resB, self.kpad, int(self.row_base[i]),
+            r.launch(self.ion_bits[i], self.n_mod, self._c[0], self.resA, self.resB, self.kpad, int(self.row_base[i]),
                      self.rows_alloc, self.rowscale, self.left, self.right, self.cbound, self.cwp, self.xwork, ls)
         for ls in used:
             join = torch.cuda.Event()
@@ -200,9 +218,9 @@ class SplitBatch(_Graphable):
                                            _native.stream_handle(stream)),
                       "rkb_split_contract")
 
-    def step(self, stream=None) -> None:
+    def step(self, stream=None, side_streams=None) -> None:
         """Enqueue every row launch and the one contraction (no host sync)."""
-        self.rows(stream)
+        self.rows(stream, side_streams)
         self.contract(stream)
 
     def check_status(self) -> None:
@@ -237,7 +255,8 @@ class SplitBatch(_Graphable):
                         info={"bits": self.bits, "n_mod": self.n_mod, "fused": self.ions[ion].fused})
 
     def info(self) -> dict:
-        return {"ions": len(self.devs), "bits": self.bits, "n_mod": self.n_mod, "kpad": self.kpad,
+        return {"ions": len(self.devs), "bits": self.bits, "ion_bits": sorted(set(self.ion_bits)),
+                "n_mod": self.n_mod, "kpad": self.kpad,
                 "order": self.order, "tasks": self.n_tasks, "rows": int(self.row_base[-1]),
                 "cert_limit": self.cert_limit, "fp64_tables": [list(t) for t in self.escalated],
                 "row_kernels": {kd: sum(r.kind == kd for r in self.ions) for kd in ("cells", "fused", "two")},

@@ -566,7 +566,9 @@ def serve_leg(args) -> dict:
     out = {"requests": len(stream), "rate_per_s": 200.0, "arrival_span_s": stream[-1][0],
            "sink": "device: per-(k, row) sums of every multipole table",
            "p99_bound_ms": P99_BOUND_MS,
-           "note": "latency = last table delivered - arrival (server clock), realtime Poisson arrivals"}
+           "note": "latency = last table delivered - arrival (server clock), realtime Poisson arrivals; "
+                   "requests ready together run as one group (one batched contraction launch) in one of "
+                   f"{args.serve_slots} stream slots"}
     for precision in ("split", "fp64"):
         reqs = [Request(rid=i, ion=ion, k_max=spec.k_max, arrival=t)
                 for i, ((t, spec), ion) in enumerate(zip(stream, ions))]
@@ -908,7 +910,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64-engine comparison leg")
     ap.add_argument("--serve", type=int, default=300, help="requests in the serving leg (0 = skip)")
-    ap.add_argument("--serve-slots", type=int, default=2, help="requests on the GPU at once in the serving leg")
+    ap.add_argument("--serve-slots", type=int, default=2, help="request groups on the GPU at once in the serving leg")
     ap.add_argument("--no-grid", action="store_true", help="skip the arbitrary-grid Y^k leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-ion batch leg")
     ap.add_argument("--no-stream", action="store_true", help="skip the streamed Z=54 CI table leg")

@@ -1,10 +1,11 @@
 """Serving loop: continuous batching of Slater-table requests on one GPU.
 
 A seeded Poisson stream of small requests (the serving workload's ranges,
-clipped so the test stays short) runs through the server with several
-requests in flight, and then each request alone. Every table of every request
-must be identical in both runs, since no request's work depends on another's.
-The report carries p50/p99 latency and throughput.
+clipped so the test stays short) runs through the server in one group, in
+several groups in flight at once, and then each request alone. Every table of
+every request must be identical in all runs, since no request's work depends
+on another's. The report carries p50/p99 latency, throughput and the group
+sizes.
 """
 import pytest
 
@@ -31,27 +32,58 @@ def _requests(n=10, seed=4200):
 
 @pytest.mark.parametrize("precision", ["split", "fp64"])
 def test_results_alone_equal_results_in_the_mix(precision):
+    """Every request in one group of ten (one contraction launch), in groups
+    of three on four slots at once, and alone: identical tables."""
     from atomx_b200.serve import Request, SlaterServer
-    reqs = [r for r, _ in _requests()]
-    for r in reqs:
-        r.sink = _Collect()
-    server = SlaterServer(precision=precision, max_inflight=4)
-    rep = server.serve(reqs, realtime=False)  # all at once: the mix is as dense as it gets
-    torch.cuda.synchronize()
-    assert all(r.error is None for r in reqs), [r.error for r in reqs]
-    assert rep.max_inflight_seen > 1
-    summ = rep.summary()
-    assert summ["p99_ms"] >= summ["p50_ms"] > 0 and summ["throughput_entries_per_s"] > 0
+    runs = []
+    for max_group in (16, 3):
+        reqs = [r for r, _ in _requests()]
+        for r in reqs:
+            r.sink = _Collect()
+        server = SlaterServer(precision=precision, max_inflight=4, max_group=max_group)
+        rep = server.serve(reqs, realtime=False)  # all at once: the mix is as dense as it gets
+        server.close()
+        torch.cuda.synchronize()
+        assert all(r.error is None for r in reqs), [r.error for r in reqs]
+        assert rep.max_inflight_seen > 1
+        summ = rep.summary()
+        assert summ["p99_ms"] >= summ["p50_ms"] > 0 and summ["throughput_entries_per_s"] > 0
+        assert rep.group_sizes == ([10] if max_group == 16 else [3, 3, 3, 1]), rep.group_sizes
+        runs.append(reqs)
     alone_server = SlaterServer(precision=precision, max_inflight=1)
-    for r in reqs:
+    for i, r in enumerate(runs[0]):
         solo = Request(rid=r.rid, ion=r.ion, k_max=r.k_max, sink=_Collect())
         alone_server.serve([solo], realtime=False)
         torch.cuda.synchronize()
-        assert sorted(solo.sink.tables) == sorted(r.sink.tables)
-        for k, t in r.sink.tables.items():
-            assert torch.equal(t, solo.sink.tables[k]), (r.rid, k)
-    server.close()
+        for mix in runs:
+            tabs = mix[i].sink.tables
+            assert sorted(solo.sink.tables) == sorted(tabs)
+            for k, t in tabs.items():
+                assert torch.equal(t, solo.sink.tables[k]), (r.rid, k)
     alone_server.close()
+
+
+def test_streamed_request_agrees_with_its_grouped_run():
+    """A request above group_bytes runs alone on the streaming engine; its
+    tables agree with the grouped run to the split's rounding (both are
+    within the split gate of the FP64 engine)."""
+    from atomx_b200.serve import Request, SlaterServer
+    (r, _), = _requests(n=1, seed=4204)
+    r.sink = _Collect()
+    grouped = SlaterServer(precision="split", max_inflight=1)
+    grouped.serve([r], realtime=False)
+    grouped.close()
+    s = Request(rid=0, ion=r.ion, k_max=r.k_max, sink=_Collect())
+    streamed = SlaterServer(precision="split", max_inflight=1, group_bytes=1)
+    rep = streamed.serve([s], realtime=False)
+    streamed.close()
+    torch.cuda.synchronize()
+    assert s.error is None and r.error is None and rep.group_sizes == [1]
+    assert sorted(s.sink.tables) == sorted(r.sink.tables)
+    for k, t in r.sink.tables.items():
+        u = s.sink.tables[k]
+        d = torch.diagonal(t).abs().sqrt()
+        assert float(((t - u).abs() / torch.outer(d, d)).max()) <= 1e-10, k
 
 
 def test_realtime_stream_reports_latency_and_admits_by_memory():
@@ -73,21 +105,32 @@ def test_realtime_stream_reports_latency_and_admits_by_memory():
     small.close()
 
 
-def test_served_cancelling_ion_is_within_the_gate():
+class _Replacing(_Collect):
+    """A sink that keeps one table per multipole: the server delivers every
+    table without waiting for the certificate and delivers a table that
+    failed it again, recomputed in FP64."""
+    replaces_tables = True
+
+
+@pytest.mark.parametrize("sink", [_Collect, _Replacing])
+@pytest.mark.parametrize("max_group", [16, 1])
+def test_served_cancelling_ion_is_within_the_gate(sink, max_group):
     """A request whose k=7 table fails the split certificate (ion 42 of the
-    uneven batch) served in a mix: its streamed tables take the FP64 route
-    and every table is within 1e-10 (Schwarz-relative) of the FP64 engine."""
+    uneven batch) served in a mix, in a group or in a slot of its own: its
+    k=7 table takes the FP64 route (before delivery, or delivered again) and
+    every table is within 1e-10 (Schwarz-relative) of the FP64 engine."""
     from atomx_b200 import workloads as W
     from atomx_b200.serve import Request, SlaterServer
     from atomx_b200.tables import tables_for, upload_ion
     spec = W.uneven_batch()[42]
     ion = W.build_ion(spec)
-    target = Request(rid=99, ion=ion, k_max=spec.k_max, sink=_Collect())
+    target = Request(rid=99, ion=ion, k_max=spec.k_max, sink=sink())
     others = [r for r, _ in _requests(n=4, seed=4203)]
     for r in others:
-        r.sink = _Collect()
-    server = SlaterServer(precision="split", max_inflight=4)
-    server.serve([target] + others, realtime=False)
+        r.sink = sink()
+    server = SlaterServer(precision="split", max_inflight=4, max_group=max_group)
+    rep = server.serve([target] + others, realtime=False)
+    assert rep.fp64_tables >= 1
     torch.cuda.synchronize()
     assert target.error is None and all(r.error is None for r in others)
     plain = tables_for(upload_ion(ion, k_max=spec.k_max), "fp64")

@@ -135,6 +135,56 @@ def test_serving_footprint_grows_with_the_request():
     assert 0 < fs < fb and ff > 0
     # the split estimate covers the residue matrices of that ion (11 moduli, two copies)
     assert fb > 2 * 11 * 56209 * 1024
+    # held whole (a request in a group), the Z=70 tables add their 2.5 GB
+    whole = footprint_bytes(big, PL.make_plan(big.kappa, 12), "split", whole_tables=True)
+    assert whole - fb > 8 * 318112753 - 2 * 8 * 14000 ** 2
+
+
+def _req(rid, fp, streamed=False):
+    from atomx_b200.serve import Request
+    r = Request(rid=rid, ion=None, k_max=0, arrival=float(rid))
+    r.footprint, r.state["streamed"] = fp, streamed
+    return r
+
+
+def test_serving_groups_are_fifo_and_bounded():
+    """Group formation of the serving loop (no GPU): arrival order, at most
+    max_group requests and group_bytes of device memory, within the HBM
+    budget beside the groups in flight, a streamed request alone, and the
+    first request of an idle device always admitted."""
+    from collections import deque
+    from types import SimpleNamespace
+
+    from atomx_b200.serve import SlaterServer
+
+    def take(srv, q, used, busy):
+        group, fp = SlaterServer._take_group(srv, q, used, busy)
+        assert fp == sum(r.footprint for r in group)
+        return group
+
+    srv = SimpleNamespace(max_group=3, group_bytes=100, hbm_budget=1000)
+    q = deque(_req(i, 10) for i in range(5))
+    assert [r.rid for r in take(srv, q, 0, False)] == [0, 1, 2] and [r.rid for r in q] == [3, 4]
+    q = deque([_req(0, 60), _req(1, 30), _req(2, 20), _req(3, 5)])
+    assert [r.rid for r in take(srv, q, 0, False)] == [0, 1]          # 60 + 30 + 20 > group_bytes
+    q = deque([_req(0, 400), _req(1, 10)])
+    assert take(srv, q, 700, True) == [] and len(q) == 2               # budget full while busy
+    assert [r.rid for r in take(srv, q, 700, False)] == [0]            # an idle device takes the head
+    q = deque([_req(0, 10), _req(1, 500, streamed=True), _req(2, 10)])
+    assert [r.rid for r in take(srv, q, 0, False)] == [0]
+    assert [r.rid for r in take(srv, q, 0, False)] == [1]              # a streamed request runs alone
+    assert [r.rid for r in take(srv, q, 0, False)] == [2]
+
+
+def test_serving_group_rows_take_the_widest_row():
+    """In a group every ion's rows are padded to the group's widest row, and
+    the group's footprint says so."""
+    from atomx_b200.serve import _group_footprint
+    a, b = _req(0, 0), _req(1, 0)
+    a.state["parts"], b.state["parts"] = (100, 10, 256, 30), (50, 20, 1024, 30)
+    a.footprint, b.footprint = 100 + 10 * 256 * 30, 50 + 20 * 1024 * 30
+    assert _group_footprint([a]) == a.footprint
+    assert _group_footprint([a, b]) == 150 + 30 * 1024 * 30 > a.footprint + b.footprint
 
 
 def test_plan_is_cached_read_only_and_ordered():
