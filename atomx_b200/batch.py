@@ -37,7 +37,7 @@ from .split import (CB_STRIDE, CERT_LIMIT, IonRows, _round_up, certify, check_kd
 from .split_plan import crt_constants
 from .tables import TILE, Fp64Recompute, IonDevice, RkTables, tile_tasks
 
-__all__ = ["SplitBatch", "Fp64Batch", "batch_tasks"]
+__all__ = ["SplitBatch", "Fp64Batch", "Workspace", "batch_tasks"]
 
 
 def batch_tasks(sizes, costs, order: str = "lpt") -> np.ndarray:
@@ -54,6 +54,56 @@ def batch_tasks(sizes, costs, order: str = "lpt") -> np.ndarray:
     elif order != "group":
         raise ValueError(f"unknown task order {order!r}")
     return tasks
+
+
+class Workspace:
+    """Device memory a caller reuses from one batch to the next (a serving
+    slot keeps one): ``take`` carves 256-byte aligned views out of one
+    buffer, adding a chunk when a batch needs more than it holds, and
+    ``reset`` merges the chunks into one buffer for the next batch.  After a
+    few batches the largest one fits and no batch allocates device memory.
+    Views taken since the last ``reset`` are valid until the next: reset only
+    once the previous batch's work, and every sink's work on its tables, is
+    done."""
+
+    ALIGN = 256
+    MIN_CHUNK = 64 << 20
+
+    def __init__(self, device=None):
+        self.device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.chunks: list = []
+        self.pos = 0      # offset in the last chunk
+        self.taken = 0    # aligned bytes taken since the last reset
+
+    @property
+    def capacity(self) -> int:
+        return int(sum(c.numel() for c in self.chunks))
+
+    def take(self, shape, dtype) -> torch.Tensor:
+        shape = tuple(int(x) for x in (shape if isinstance(shape, (tuple, list)) else (shape,)))
+        nbytes = int(np.prod(shape, dtype=np.int64)) * torch.empty((), dtype=dtype).element_size()
+        step = -(-nbytes // self.ALIGN) * self.ALIGN
+        if not self.chunks or self.pos + step > self.chunks[-1].numel():
+            self.chunks.append(torch.empty(max(step, self.MIN_CHUNK), dtype=torch.uint8, device=self.device))
+            self.pos = 0
+        t = self.chunks[-1][self.pos:self.pos + nbytes].view(dtype).view(shape)
+        self.pos += step
+        self.taken += step
+        return t
+
+    def reset(self) -> None:
+        if len(self.chunks) > 1:
+            need = self.taken
+            self.chunks = []  # back to the caching allocator before the merged buffer is taken
+            self.chunks = [torch.empty(need, dtype=torch.uint8, device=self.device)]
+        self.pos = 0
+        self.taken = 0
+
+
+def _alloc(workspace, shape, dtype, device):
+    if workspace is None:
+        return torch.empty(shape, dtype=dtype, device=device)
+    return workspace.take(shape, dtype)
 
 
 class _Graphable:
@@ -88,7 +138,8 @@ class SplitBatch(_Graphable):
 
     def __init__(self, devs: list[IonDevice], bits: int | None = None, tau: float = 1e-3, fused=None,
                  corr_floor: float | None = None, order: str = "lpt", n_mod: int | None = None,
-                 cert_limit: float = CERT_LIMIT, ion_widths: bool = False, ion_rows: list | None = None):
+                 cert_limit: float = CERT_LIMIT, ion_widths: bool = False, ion_rows: list | None = None,
+                 workspace: Workspace | None = None):
         _native.require_device()
         if not devs:
             raise ValueError("empty batch")
@@ -117,14 +168,26 @@ class SplitBatch(_Graphable):
         self.row_base = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         nrows = int(self.row_base[-1])
         self.rows_alloc = _round_up(max(nrows, 1), TILE)
-        self.resA = torch.zeros((self.n_mod, self.rows_alloc, self.kpad), dtype=torch.int8, device=d)
-        self.resB = torch.zeros_like(self.resA) if any(r.has_z for r in self.ions) else None
-        self.rowscale = torch.empty(nrows, dtype=torch.float64, device=d)
-        self.left = torch.zeros((nrows, self.cwp), dtype=torch.float64, device=d)
-        self.right = torch.zeros_like(self.left)
-        self.cbound = torch.empty((nrows, CB_STRIDE), dtype=torch.float64, device=d)
+        ws = workspace
+        res_shape = (self.n_mod, self.rows_alloc, self.kpad)
+        self.resA = _alloc(ws, res_shape, torch.int8, d)
+        self.resB = _alloc(ws, res_shape, torch.int8, d) if any(r.has_z for r in self.ions) else None
+        # The cell and two-kernel row paths write every column of their rows;
+        # the fused kernel only its own.  Padding rows are read by the last
+        # tiles (their entries are never stored) and are zeroed all the same.
+        full_zero = any(r.kind == "fused" for r in self.ions)
+        for res in (self.resA, self.resB):
+            if res is not None:
+                (res if full_zero else res[:, nrows:, :]).zero_()
+        self.rowscale = _alloc(ws, (nrows,), torch.float64, d)
+        # core vectors: an ion writes its own ng + 2 columns of the batch's cwp
+        self.left = _alloc(ws, (nrows, self.cwp), torch.float64, d)
+        self.right = _alloc(ws, (nrows, self.cwp), torch.float64, d)
+        self.left.zero_()
+        self.right.zero_()
+        self.cbound = _alloc(ws, (nrows, CB_STRIDE), torch.float64, d)
         two = [dv.plan.n_rows for dv, r in zip(self.devs, self.ions) if r.kind == "two"]
-        self.xwork = torch.empty((max(two), self.kpad), dtype=torch.float64, device=d) if two else None
+        self.xwork = _alloc(ws, (max(two), self.kpad), torch.float64, d) if two else None
         self.corr_floor = 2.0 ** -(self.bits + 10) if corr_floor is None else float(corr_floor)
         # groups: (ion, k)
         g_row0, g_n, g_kdim, self.group_of = [], [], [], []
@@ -154,7 +217,7 @@ class SplitBatch(_Graphable):
         #: (ion, k) tables recomputed in FP64 by the last check_status()
         self.escalated: list = []
         self._stream = None
-        self.out = torch.empty(self.total, dtype=torch.float64, device=d)
+        self.out = _alloc(ws, (self.total,), torch.float64, d)
         self._c = (np.ctypeslib.as_ctypes(np.ascontiguousarray(self.moduli, dtype=np.int32)),
                    np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_hi)),
                    np.ctypeslib.as_ctypes(np.ascontiguousarray(self.f_lo)),
@@ -268,7 +331,7 @@ class Fp64Batch(_Graphable):
 
     dominant_kernel = "fp64tab::contract_kernel"
 
-    def __init__(self, devs: list[IonDevice], order: str = "lpt"):
+    def __init__(self, devs: list[IonDevice], order: str = "lpt", workspace: Workspace | None = None):
         _native.require_device()
         if not devs:
             raise ValueError("empty batch")
@@ -278,8 +341,8 @@ class Fp64Batch(_Graphable):
         counts = [dv.plan.n_rows for dv in self.devs]
         self.row_base = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         nrows = int(self.row_base[-1])
-        self.g = torch.empty((nrows, self.ld), dtype=torch.float64, device=d)
-        self.y = torch.empty_like(self.g)
+        self.g = _alloc(workspace, (nrows, self.ld), torch.float64, d)
+        self.y = _alloc(workspace, (nrows, self.ld), torch.float64, d)
         g_row0, g_n, g_kdim, self.group_of = [], [], [], []
         for i, dv in enumerate(self.devs):
             for k in dv.plan.ks:
@@ -298,7 +361,7 @@ class Fp64Batch(_Graphable):
         tasks = batch_tasks(g_n, g_kdim, order)
         self.n_tasks = int(tasks.shape[0])
         self.tasks = torch.as_tensor(tasks.reshape(-1), device=d)
-        self.out = torch.empty(self.total, dtype=torch.float64, device=d)
+        self.out = _alloc(workspace, (self.total,), torch.float64, d)
 
     @property
     def launches_per_step(self) -> int:

@@ -19,7 +19,8 @@ R^k tables. The server runs each request through three stages:
 3. device work, on the slot's CUDA stream and set up by the slot's launcher
    thread: every ion's row kernels (spread over the slot's side streams) and
    ONE contraction launch over the tiles of every (ion, k) table of the group
-   (``batch.SplitBatch`` / ``batch.Fp64Batch``). Each table then goes to its
+   (``batch.SplitBatch`` / ``batch.Fp64Batch``, their buffers carved from the
+   slot's reusable ``batch.Workspace``). Each table then goes to its
    request's sink with its kappa-block ranges. The launcher waits (without
    the GIL) for an event after the last table, completes the group (for
    sinks that take a table again, tables whose split certificate failed are
@@ -55,7 +56,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from .batch import Fp64Batch, SplitBatch
+from .batch import Fp64Batch, SplitBatch, Workspace
 from .plan import make_plan
 from .split import KDIM_MAX, IonRows, check_kdim, host_tables
 from .split_plan import bits_for_moduli, moduli_needed
@@ -191,10 +192,13 @@ def _group_footprint(reqs) -> int:
 
 @dataclass
 class _Slot:
-    """A stream slot: the stream a group runs on and the side streams its
-    row kernels spread over."""
+    """A stream slot: the stream a group runs on, the side streams its row
+    kernels spread over, and the device workspace its batches reuse (tables,
+    residues and rows of one group at a time, so groups after the first few
+    allocate no device memory)."""
     stream: object
     side: list
+    ws: object
 
 
 class SlaterServer:
@@ -223,7 +227,7 @@ class SlaterServer:
         # run there, and the thread then waits (without the GIL) for the
         # group's completion event, so the loop itself only admits and retires
         self.launchers = ThreadPoolExecutor(max_workers=self.max_inflight)
-        self.slots = [_Slot(torch.cuda.Stream(), [torch.cuda.Stream() for _ in range(ROW_STREAMS)])
+        self.slots = [_Slot(torch.cuda.Stream(), [torch.cuda.Stream() for _ in range(ROW_STREAMS)], Workspace())
                       for _ in range(self.max_inflight)]
         self._tls = threading.local()  # per planner thread: its CUDA stream
         self._t0 = time.perf_counter()
@@ -286,14 +290,17 @@ class SlaterServer:
         certificates)."""
         s = slot.stream
         devs = [self._dev(r, s) for r in group]
+        # the slot's previous group, and its sinks' work, completed before
+        # this launcher returned: its workspace views are free again
+        slot.ws.reset()
         split = self.precision == "split"
         if split:
             rows = [r.state.get("ion_rows") for r in group]
             b = SplitBatch(devs, bits=self.bits, n_mod=SERVE_N_MOD, ion_widths=True, corr_floor=SERVE_CORR_FLOOR,
-                           ion_rows=rows if all(x is not None for x in rows) else None)
+                           ion_rows=rows if all(x is not None for x in rows) else None, workspace=slot.ws)
             b.step(s, slot.side)
         else:
-            b = Fp64Batch(devs)
+            b = Fp64Batch(devs, workspace=slot.ws)
             b.step(s)
         deferred = split and all(getattr(r.sink, "replaces_tables", False) for r in group)
         if split and not deferred:

@@ -123,6 +123,35 @@ def test_host_tables_equal_the_per_multipole_factors(name, ks, threads, monkeypa
     SP._host_cache.clear()
 
 
+def test_workspace_views_are_aligned_disjoint_and_merge_on_reset():
+    """The reusable batch workspace (exercised on host memory): aligned,
+    non-overlapping views of the requested shapes; a batch that outgrows it
+    adds a chunk, and reset merges the chunks so the next batch of the same
+    size takes no new memory."""
+    import torch
+
+    from atomx_b200.batch import Workspace
+    ws = Workspace(device=torch.device("cpu"))
+    ws.MIN_CHUNK = 4096
+    shapes = [((3, 5, 128), torch.int8), ((7,), torch.float64), ((9, 14), torch.float64), ((3000,), torch.float64)]
+    for rnd in range(3):
+        views = [ws.take(sh, dt) for sh, dt in shapes]
+        spans = []
+        for v, (sh, dt) in zip(views, shapes):
+            assert tuple(v.shape) == sh and v.dtype == dt and v.is_contiguous()
+            base = [c.data_ptr() for c in ws.chunks if c.data_ptr() <= v.data_ptr() < c.data_ptr() + c.numel()]
+            assert len(base) == 1 and (v.data_ptr() - base[0]) % Workspace.ALIGN == 0  # (device chunks: 512-aligned)
+            spans.append((v.data_ptr(), v.data_ptr() + v.numel() * v.element_size()))
+            v.fill_(rnd + 1)
+        spans.sort()
+        assert all(a[1] <= b[0] for a, b in zip(spans, spans[1:]))
+        assert all(bool((v == rnd + 1).all()) for v in views)
+        ws.reset()
+        if rnd == 0:
+            merged = ws.capacity
+        assert len(ws.chunks) == 1 and ws.capacity == merged
+
+
 def test_serving_footprint_grows_with_the_request():
     from atomx_b200 import plan as PL
     from atomx_b200 import workloads as W
