@@ -45,15 +45,15 @@ def batch_tasks(sizes, costs, order: str = "lpt") -> np.ndarray:
 
     ``costs[g]`` is the relative cost of one tile of group g (its
     contraction length). "lpt" puts the most expensive tiles first (persistent
-    CTAs then finish close together); "group" keeps groups in order.
+    CTAs then finish close together): groups by decreasing cost, ties in
+    group order, each group's tiles row-major; "group" keeps groups in order.
     """
-    tasks = tile_tasks(sizes)
-    if order == "lpt" and tasks.shape[0]:
-        c = np.asarray(costs, dtype=np.float64)[tasks[:, 0]]
-        tasks = tasks[np.argsort(-c, kind="stable")]
-    elif order != "group":
+    if order == "lpt":
+        c = np.asarray(costs, dtype=np.float64).reshape(-1)
+        return tile_tasks(sizes, order=np.argsort(-c, kind="stable"))
+    if order != "group":
         raise ValueError(f"unknown task order {order!r}")
-    return tasks
+    return tile_tasks(sizes)
 
 
 class Workspace:

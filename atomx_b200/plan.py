@@ -70,7 +70,7 @@ class TablePlan:
             else:
                 starts = np.concatenate([[0], np.flatnonzero(bid[1:] != bid[:-1]) + 1])
                 stops = np.concatenate([starts[1:], [bid.shape[0]]])
-                hit = tuple((int(bid[a]), int(a), int(b)) for a, b in zip(starts, stops))
+                hit = tuple(zip(bid[starts].tolist(), starts.tolist(), stops.tolist()))
             cache[k] = hit
         return list(hit)
 

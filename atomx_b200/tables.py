@@ -18,6 +18,7 @@ Precision forms:
 from __future__ import annotations
 
 from dataclasses import dataclass, field
+from functools import lru_cache
 
 import numpy as np
 import torch
@@ -121,18 +122,27 @@ def upload_values(Pv, Qv, kappa, gr, grw, k_max: int, plan: TablePlan | None = N
                      extra={"r_host": None if isinstance(gr, torch.Tensor) else np.asarray(gr, dtype=np.float64).reshape(-1)})
 
 
-def tile_tasks(sizes, tile: int = TILE):
-    """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes
-    (each group's tiles row-major, groups in order)."""
+@lru_cache(maxsize=512)
+def _triangle(nt: int) -> np.ndarray:
+    """(2, nt (nt + 1) / 2) int32: the row-major upper triangle of nt x nt tiles."""
+    t = np.stack(np.triu_indices(nt)).astype(np.int32)
+    t.setflags(write=False)
+    return t
+
+
+def tile_tasks(sizes, tile: int = TILE, order=None):
+    """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes:
+    each group's tiles row-major, groups in order (or in the group order
+    ``order``, a permutation of the group indices)."""
     nt = (np.asarray(sizes, dtype=np.int64).reshape(-1) + tile - 1) // tile
-    if nt.shape[0] == 0 or not nt.any():
+    groups = np.arange(nt.shape[0]) if order is None else np.asarray(order, dtype=np.int64)
+    groups = groups[nt[groups] > 0]
+    if groups.shape[0] == 0:
         return np.zeros((0, 3), dtype=np.int32)
-    # row-major upper triangle of the largest group; a group of nt tiles per
-    # side takes the entries with tj < nt, in the same order
-    ti, tj = np.triu_indices(int(nt.max()))
-    keep = tj[None, :] < nt[:, None]                      # (groups, triangle)
-    g, e = np.nonzero(keep)
-    return np.stack([g, ti[e], tj[e]], axis=1).astype(np.int32)
+    tri = [_triangle(int(n)) for n in nt[groups]]
+    g = np.repeat(groups.astype(np.int32), [t.shape[1] for t in tri])
+    tt = np.concatenate(tri, axis=1)
+    return np.stack([g, tt[0], tt[1]], axis=1)
 
 
 @dataclass
