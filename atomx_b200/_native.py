@@ -47,6 +47,7 @@ _SIGNATURES = {
     "rkb_split_fused_body_width": [_i, _i],
     "rkb_green_factor": [_vp, _i, _i, _i, _d, _vp, _vp, _vp, _l],
     "rkb_green_tables": [_vp, _i, _i, _vp, _i, _d, _vp, _vp, _i, _i, _vp, _l, _vp, _vp, _l, _vp, _vp],
+    "rkb_table_plan": [_vp, _vp, _i, _vp, _i, _l, _l, _vp, _vp, _vp, _vp],
     "rkb_split_certify": [_vp, _vp, _l, _vp, _vp, _d, _vp, _vp, _vp],
     "rkb_occupied_density": [_vp, _vp, _l, _l, _vp, _l, _l, _vp, _vp],
     "rkb_bspline_sym_matrix": [_vp, _i, _vp, _i, _i, _i, _vp, _vp, _l, _vp, _vp],
@@ -68,7 +69,7 @@ _SIGNATURES = {
                            _vp, _vp, _vp, _l, _vp, _vp, _vp],
 }
 _RESTYPE = {"rkb_last_error": _c.c_char_p, "rkb_version": _c.c_char_p, "rkb_split_fused_body_width": _c.c_long,
-            "rkb_green_factor": _c.c_long, "rkb_green_tables": _c.c_long, "rkb_gauss_legendre_01": None}
+            "rkb_green_factor": _c.c_long, "rkb_green_tables": _c.c_long, "rkb_table_plan": _c.c_long, "rkb_gauss_legendre_01": None}
 
 _lock = threading.Lock()
 _lib = None

@@ -266,3 +266,47 @@ extern "C" long rkb_green_tables(const double *r, int nv, int ng, const int *ks,
     }
     return pos;
 }
+
+// Table plan of an orbital set, filled natively (the caller sizes it): pairs
+// a <= c by kappa-shell blocks (shell pairs i <= j, i-major; inside a block
+// a-major, a <= c within one shell), then the rows (pair, k) grouped by k in
+// increasing order, each k's pairs ascending.
+extern "C" long rkb_table_plan(const long *shell_start, const long *shell_size, int n_shells,
+                               const unsigned char *allowed, int k_max, long n_pairs, long n_rows, long *pairs,
+                               long *pair_block, long *row_pair, long *row_k) {
+    RKB_CHECK_ARG(shell_start != nullptr && shell_size != nullptr && allowed != nullptr && pairs != nullptr &&
+                      pair_block != nullptr && row_pair != nullptr && row_k != nullptr,
+                  "null argument");
+    RKB_CHECK_ARG(n_shells >= 1 && k_max >= 0 && n_pairs >= 0 && n_rows >= 0, "invalid plan sizes");
+    const long nb = (long)n_shells * (n_shells + 1) / 2;
+    std::vector<long> boff((size_t)nb + 1);
+    long p = 0, b = 0;
+    for (int i = 0; i < n_shells; ++i)
+        for (int j = i; j < n_shells; ++j, ++b) {
+            boff[(size_t)b] = p;
+            const long na = shell_size[i], nc = shell_size[j], a0 = shell_start[i], c0 = shell_start[j];
+            const long need = i == j ? na * (na + 1) / 2 : na * nc;
+            RKB_CHECK_ARG(na >= 0 && nc >= 0 && p + need <= n_pairs, "pair count %ld exceeded", n_pairs);
+            for (long a = 0; a < na; ++a)
+                for (long c = (i == j ? a : 0); c < nc; ++c, ++p) {
+                    pairs[2 * p] = a0 + a;
+                    pairs[2 * p + 1] = c0 + c;
+                    pair_block[p] = b;
+                }
+        }
+    boff[(size_t)nb] = p;
+    RKB_CHECK_ARG(p == n_pairs, "the shells give %ld pairs, not %ld", p, n_pairs);
+    long q = 0;
+    for (int k = 0; k <= k_max; ++k)
+        for (long blk = 0; blk < nb; ++blk) {
+            if (!allowed[blk * (k_max + 1) + k]) continue;
+            const long s = boff[(size_t)blk], e = boff[(size_t)blk + 1];
+            RKB_CHECK_ARG(q + (e - s) <= n_rows, "row count %ld exceeded", n_rows);
+            for (long t = s; t < e; ++t, ++q) {
+                row_pair[q] = t;
+                row_k[q] = k;
+            }
+        }
+    RKB_CHECK_ARG(q == n_rows, "the allowed multipoles give %ld rows, not %ld", q, n_rows);
+    return q;
+}

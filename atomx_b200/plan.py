@@ -22,6 +22,8 @@ from functools import lru_cache
 
 import numpy as np
 
+from . import _native
+
 from .angular import exchange_k_range
 
 __all__ = ["TablePlan", "make_plan"]
@@ -108,20 +110,6 @@ def _allowed_mask(kappa_a: int, kappa_c: int, k_max: int) -> tuple:
     return tuple(k in al for k in range(k_max + 1))
 
 
-def _triu_rows(l: np.ndarray, n: np.ndarray):
-    """(row, col) of position l in the a-major upper triangle (diagonal
-    included) of an n x n block: row i starts at i n - i (i - 1) / 2."""
-    b = 2 * n + 1
-    i = np.floor((b - np.sqrt(b.astype(np.float64) ** 2 - 8.0 * l)) / 2.0).astype(np.int64)
-    for _ in range(2):  # guard the square root's rounding
-        start = i * n - i * (i - 1) // 2
-        i = np.where(start > l, i - 1, i)
-        nxt = (i + 1) * n - (i + 1) * i // 2
-        i = np.where(nxt <= l, i + 1, i)
-    start = i * n - i * (i - 1) // 2
-    return i, i + (l - start)
-
-
 def _make_plan(kappa, k_max: int) -> TablePlan:
     n = kappa.shape[0]
     if n == 0:
@@ -135,31 +123,30 @@ def _make_plan(kappa, k_max: int) -> TablePlan:
     skap = kappa[starts]
     # Blocks: shell pairs (i <= j) in i-major order; pairs a <= c within a shell, a-major.
     si, sj = np.triu_indices(starts.shape[0])
-    same = si == sj
     na, nc = sizes[si], sizes[sj]
-    bsize = np.where(same, na * (na + 1) // 2, na * nc)
+    bsize = np.where(si == sj, na * (na + 1) // 2, na * nc)
     boff = np.concatenate([[0], np.cumsum(bsize)]).astype(np.int64)
-    total = int(boff[-1])
-    bid = np.repeat(np.arange(si.shape[0]), bsize)
-    loc = np.arange(total, dtype=np.int64) - boff[bid]
-    ncb = nc[bid]
-    a_loc, c_loc = loc // ncb, loc % ncb
-    sm = same[bid]
-    if sm.any():
-        a_loc[sm], c_loc[sm] = _triu_rows(loc[sm], na[bid][sm])
-    pairs = np.stack([starts[si][bid] + a_loc, starts[sj][bid] + c_loc], axis=1).astype(np.int64)
-    pblock = bid.astype(np.int64)
-    allowed = np.array([_allowed_mask(int(skap[a]), int(skap[b]), int(k_max)) for a, b in zip(si, sj)],
-                       dtype=bool).reshape(si.shape[0], k_max + 1)
-    blocks = [(int(skap[a]), int(skap[b]), int(boff[t]), int(boff[t + 1])) for t, (a, b) in enumerate(zip(si, sj))]
-    ks = [int(k) for k in np.flatnonzero(allowed.any(axis=0))]
-    pairs_of_k = {k: np.flatnonzero(allowed[pblock, k]).astype(np.int64) for k in ks}
-    off, pos = {}, 0
+    allowed = np.array([_allowed_mask(a, c, int(k_max)) for a, c in zip(skap[si].tolist(), skap[sj].tolist())],
+                       dtype=np.uint8).reshape(si.shape[0], k_max + 1)
+    per_k = bsize @ allowed.astype(np.int64)             # rows of each k
+    ks = np.flatnonzero(per_k).tolist()
+    n_pairs, n_rows = int(boff[-1]), int(per_k.sum())
+    pairs = np.empty((n_pairs, 2), dtype=np.int64)
+    pblock = np.empty(n_pairs, dtype=np.int64)
+    row_pair = np.empty(n_rows, dtype=np.int64)
+    row_k = np.empty(n_rows, dtype=np.int64)
+    allowed = np.ascontiguousarray(allowed)
+    # the pair and row arrays, filled natively (no interpreter lock held)
+    got = _native.load().rkb_table_plan(starts.ctypes.data, sizes.ctypes.data, int(starts.shape[0]),
+                                        allowed.ctypes.data, int(k_max), n_pairs, n_rows, pairs.ctypes.data,
+                                        pblock.ctypes.data, row_pair.ctypes.data, row_k.ctypes.data)
+    if got < 0:
+        _native.check(int(-got), "rkb_table_plan")
+    blocks = list(zip(skap[si].tolist(), skap[sj].tolist(), boff[:-1].tolist(), boff[1:].tolist()))
+    off, pairs_of_k, pos = {}, {}, 0
     for k in ks:
         off[k] = pos
-        pos += pairs_of_k[k].shape[0]
-    row_pair = np.concatenate([pairs_of_k[k] for k in ks]) if ks else np.zeros(0, np.int64)
-    row_k = np.concatenate([np.full(pairs_of_k[k].shape[0], k, dtype=np.int64) for k in ks]) if ks else \
-        np.zeros(0, np.int64)
+        pairs_of_k[k] = row_pair[pos:pos + int(per_k[k])]
+        pos += int(per_k[k])
     return TablePlan(kappa=kappa, pairs=pairs, pair_block=pblock, blocks=blocks, ks=ks,
-                     pairs_of_k=pairs_of_k, row_pair=row_pair.astype(np.int64), row_k=row_k, k_row_offset=off)
+                     pairs_of_k=pairs_of_k, row_pair=row_pair, row_k=row_k, k_row_offset=off)

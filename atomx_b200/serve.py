@@ -239,6 +239,8 @@ class SlaterServer:
     def _plan(self, req: Request) -> Request:
         t0 = time.perf_counter()
         req.plan = make_plan(req.ion.kappa, req.k_max)
+        for k in req.plan.ks:  # the sinks' kappa-block ranges, built here rather than by the launcher
+            req.plan.block_ranges_of_k(k)
         if self.precision == "split":
             host_tables(np.asarray(req.ion.bsp["gr"], dtype=np.float64).reshape(-1), req.ion.bsp["gr"].shape[1],
                         req.plan.ks)

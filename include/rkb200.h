@@ -308,6 +308,20 @@ long rkb_green_tables(const double *r, int nv, int ng, const int *ks, int nk, do
                       const double *mi, int nthreads, int kmax, double *flat, long flat_cap, long *koff,
                       double *flat_t, long flat_t_cap, long *koff_t, long *nz);
 
+/* Host-only planning: the table plan of an orbital set, sized by the caller.
+ * n_shells kappa shells (maximal runs of equal kappa in orbital order) start
+ * at shell_start[s] with shell_size[s] orbitals; allowed[b][k] (k <= k_max)
+ * marks the multipoles the angular rules allow for shell pair b (pairs i <= j
+ * in i-major order).  Writes pairs[n_pairs][2] (a <= c by shell-pair block,
+ * a-major inside a block), pair_block[n_pairs], and the rows (pair, k)
+ * grouped by k in increasing order, each k's pairs ascending: row_pair and
+ * row_k[n_rows].  Returns n_rows or a negative rkb_status when the counts
+ * disagree.  Follows the pair and row order of atomx_b200.plan, which orders
+ * atomx's exchange_k_range selection (atomx angular rules) into tables. */
+long rkb_table_plan(const long *shell_start, const long *shell_size, int n_shells, const unsigned char *allowed,
+                    int k_max, long n_pairs, long n_rows, long *pairs, long *pair_block, long *row_pair,
+                    long *row_k);
+
 /* Residue positions spanned by the body in rkb_split_rows_fused's layout (a
  * multiple of 128), or -1 for an invalid grid.  Host-only, no device work. */
 long rkb_split_fused_body_width(int nv, int ng);
