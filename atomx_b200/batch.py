@@ -91,6 +91,16 @@ class Workspace:
         self.taken += step
         return t
 
+    def reserve(self, nbytes: int) -> None:
+        """Hold at least ``nbytes`` in one buffer from now on (call between
+        batches, with nothing taken)."""
+        if self.taken:
+            raise RuntimeError("reserve() with views taken; call reset() first")
+        if self.capacity < nbytes or len(self.chunks) > 1:
+            self.chunks = []
+            self.chunks = [torch.empty(max(int(nbytes), self.capacity), dtype=torch.uint8, device=self.device)]
+        self.pos = 0
+
     def reset(self) -> None:
         if len(self.chunks) > 1:
             need = self.taken

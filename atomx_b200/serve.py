@@ -7,7 +7,7 @@ R^k tables. The server runs each request through three stages:
 1. planning, in a worker pool: the pair/row plan and, for the split engine,
    the factored Green operators of the grid and their packed host tables
    (one native call, cached by grid content); then the request's device
-   inputs, staged on the planner thread's own stream (coefficients, orbital
+   inputs, staged on the planners' staging stream (coefficients, orbital
    values, basis and plan arrays, the split engine's factor tables);
 2. admission in groups: when a stream slot is free, the requests at the head
    of the ready queue (arrival order) form the next group while it holds at
@@ -229,7 +229,7 @@ class SlaterServer:
         self.launchers = ThreadPoolExecutor(max_workers=self.max_inflight)
         self.slots = [_Slot(torch.cuda.Stream(), [torch.cuda.Stream() for _ in range(ROW_STREAMS)], Workspace())
                       for _ in range(self.max_inflight)]
-        self._tls = threading.local()  # per planner thread: its CUDA stream
+        self._stage_stream, self._stage_lock = None, threading.Lock()
         self._t0 = time.perf_counter()
 
     def _now(self) -> float:
@@ -258,15 +258,18 @@ class SlaterServer:
         return req
 
     def _planner_stream(self):
-        st = getattr(self._tls, "stream", None)
-        if st is None:
-            with torch.cuda.device(self.device):
-                st = self._tls.stream = torch.cuda.Stream()
-        return st
+        # one staging stream for every planner thread: the caching allocator
+        # keeps freed blocks per stream, so staged inputs then share one pool
+        if self._stage_stream is None:
+            with self._stage_lock:
+                if self._stage_stream is None:
+                    with torch.cuda.device(self.device):
+                        self._stage_stream = torch.cuda.Stream()
+        return self._stage_stream
 
     def _stage(self, req: Request) -> None:
         """A request's device inputs, prepared by its planner thread on the
-        planner's own stream, off the launch path: coefficients, orbital
+        staging stream, off the launch path: coefficients, orbital
         values (K1), the basis and plan arrays, and for the split engine the
         ion's row side (factor tables on the device).  A new radial grid
         makes these host-to-device copies that would otherwise stall the
@@ -293,8 +296,12 @@ class SlaterServer:
         s = slot.stream
         devs = [self._dev(r, s) for r in group]
         # the slot's previous group, and its sinks' work, completed before
-        # this launcher returned: its workspace views are free again
+        # this launcher returned: its workspace views are free again.  The
+        # first group reserves the slot's share of the budget in one buffer,
+        # so later groups allocate nothing.
         slot.ws.reset()
+        if not slot.ws.chunks:
+            slot.ws.reserve(min(self.group_bytes, self.hbm_budget // self.max_inflight))
         split = self.precision == "split"
         if split:
             rows = [r.state.get("ion_rows") for r in group]
@@ -482,3 +489,5 @@ class SlaterServer:
     def close(self):
         self.pool.shutdown(wait=True)
         self.launchers.shutdown(wait=True)
+        for slot in self.slots:  # the workspaces go back to the caching allocator
+            slot.ws.chunks = []

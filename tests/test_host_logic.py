@@ -150,6 +150,11 @@ def test_workspace_views_are_aligned_disjoint_and_merge_on_reset():
         if rnd == 0:
             merged = ws.capacity
         assert len(ws.chunks) == 1 and ws.capacity == merged
+    ws.reserve(3 * merged)
+    assert len(ws.chunks) == 1 and ws.capacity == 3 * merged
+    ws.take((10,), torch.float64)
+    with pytest.raises(RuntimeError):
+        ws.reserve(1)
 
 
 def test_serving_footprint_grows_with_the_request():
