@@ -229,6 +229,14 @@ class SlaterServer:
         self.launchers = ThreadPoolExecutor(max_workers=self.max_inflight)
         self.slots = [_Slot(torch.cuda.Stream(), [torch.cuda.Stream() for _ in range(ROW_STREAMS)], Workspace())
                       for _ in range(self.max_inflight)]
+        # each slot holds its share of the budget in one buffer from the start,
+        # so no group allocates device memory (a slow cudaMalloc, or a flush
+        # of the allocator's cache, happens here and not under a request)
+        reserve = min(self.group_bytes, self.hbm_budget // self.max_inflight)
+        if reserve >= Workspace.MIN_CHUNK:
+            for slot in self.slots:
+                with torch.cuda.stream(slot.stream):
+                    slot.ws.reserve(reserve)
         self._stage_stream, self._stage_lock = None, threading.Lock()
         self._t0 = time.perf_counter()
 
@@ -296,12 +304,8 @@ class SlaterServer:
         s = slot.stream
         devs = [self._dev(r, s) for r in group]
         # the slot's previous group, and its sinks' work, completed before
-        # this launcher returned: its workspace views are free again.  The
-        # first group reserves the slot's share of the budget in one buffer,
-        # so later groups allocate nothing.
+        # this launcher returned: its workspace views are free again
         slot.ws.reset()
-        if not slot.ws.chunks:
-            slot.ws.reserve(min(self.group_bytes, self.hbm_budget // self.max_inflight))
         split = self.precision == "split"
         if split:
             rows = [r.state.get("ion_rows") for r in group]
