@@ -217,6 +217,11 @@ class SlaterServer:
         self.max_group, self.group_bytes = int(max_group), int(group_bytes)
         if self.max_inflight < 1 or self.max_group < 1:
             raise ValueError("max_inflight and max_group must be >= 1")
+        # Blocks the caching allocator keeps for other streams (earlier work in
+        # this process) are given back first: left cached, they can fill the
+        # device under a request and force a flush (a device-wide
+        # synchronisation) mid-stream, and they would shrink the budget.
+        torch.cuda.empty_cache()
         if hbm_budget is None:
             free, total = torch.cuda.mem_get_info()
             hbm_budget = int(0.6 * free)
@@ -230,8 +235,7 @@ class SlaterServer:
         self.slots = [_Slot(torch.cuda.Stream(), [torch.cuda.Stream() for _ in range(ROW_STREAMS)], Workspace())
                       for _ in range(self.max_inflight)]
         # each slot holds its share of the budget in one buffer from the start,
-        # so no group allocates device memory (a slow cudaMalloc, or a flush
-        # of the allocator's cache, happens here and not under a request)
+        # so no group allocates device memory
         reserve = min(self.group_bytes, self.hbm_budget // self.max_inflight)
         if reserve >= Workspace.MIN_CHUNK:
             for slot in self.slots:
@@ -493,5 +497,6 @@ class SlaterServer:
     def close(self):
         self.pool.shutdown(wait=True)
         self.launchers.shutdown(wait=True)
-        for slot in self.slots:  # the workspaces go back to the caching allocator
+        for slot in self.slots:  # the workspaces go back to the device
             slot.ws.chunks = []
+        torch.cuda.empty_cache()
