@@ -60,7 +60,7 @@ from .batch import Fp64Batch, SplitBatch, Workspace
 from .plan import make_plan
 from .split import KDIM_MAX, IonRows, check_kdim, host_tables
 from .split_plan import bits_for_moduli, moduli_needed
-from .tables import upload_ion
+from .tables import stage_ion, upload_ion
 
 __all__ = ["Request", "ServeReport", "SlaterServer", "ChecksumSink", "footprint_bytes", "footprint_parts",
            "P99_BOUND_MS", "SERVE_N_MOD", "SERVE_CORR_FLOOR", "GROUP_BYTES"]
@@ -242,6 +242,7 @@ class SlaterServer:
                 with torch.cuda.stream(slot.stream):
                     slot.ws.reserve(reserve)
         self._stage_stream, self._stage_lock = None, threading.Lock()
+        self._tls = threading.local()  # per planner thread: its pinned staging buffer
         self._t0 = time.perf_counter()
 
     def _now(self) -> float:
@@ -281,17 +282,24 @@ class SlaterServer:
 
     def _stage(self, req: Request) -> None:
         """A request's device inputs, prepared by its planner thread on the
-        staging stream, off the launch path: coefficients, orbital
-        values (K1), the basis and plan arrays, and for the split engine the
-        ion's row side (factor tables on the device).  A new radial grid
-        makes these host-to-device copies that would otherwise stall the
-        launcher.  They are small beside the tables (orbital values: 16 bytes
-        per spinor and grid node)."""
+        staging stream, off the launch path (``tables.stage_ion``):
+        coefficients, the basis and plan arrays and, for the split engine,
+        the factor tables, in one device allocation and one copy from the
+        thread's pinned buffer; then the orbital values (K1) and the split
+        engine's row side.  A new radial grid would otherwise make these a
+        dozen synchronous copies on the launch path.  They are small beside
+        the tables (orbital values: 16 bytes per spinor and grid node)."""
         ps = self._planner_stream()
+        split = self.precision == "split" and not req.state["streamed"]
+        H = None
+        if split:
+            H = host_tables(np.asarray(req.ion.bsp["gr"], dtype=np.float64).reshape(-1),
+                            req.ion.bsp["gr"].shape[1], req.plan.ks)
         with torch.cuda.device(self.device), torch.cuda.stream(ps):
-            dev = upload_ion(req.ion, k_max=req.k_max, plan=req.plan, stream=ps)
-            rows = IonRows(dev) if self.precision == "split" and not req.state["streamed"] else None
-        ps.synchronize()  # the launcher's stream reads them
+            dev, dtab, pinned = stage_ion(req.ion, req.plan, ps, getattr(self._tls, "pinned", None), H)
+            rows = IonRows(dev, device_tables=dtab) if split else None
+        self._tls.pinned = pinned
+        ps.synchronize()  # the launcher's stream reads them; the pinned buffer is free again
         if rows is not None:
             check_kdim(rows.kmax_dim)  # a grid the split engine does not take fails this request alone
         req.state["dev"], req.state["ion_rows"] = dev, rows

@@ -240,7 +240,12 @@ class IonRows:
 
     KCHUNK = 128
 
-    def __init__(self, dev: IonDevice, tau: float = 1e-3, fused: bool | None = None, rows_kernel: str | None = None):
+    def __init__(self, dev: IonDevice, tau: float = 1e-3, fused: bool | None = None, rows_kernel: str | None = None,
+                 device_tables: dict | None = None):
+        """``device_tables``: the device copies of host_tables' flat, koff,
+        flat_t, koff_t and the per-k Z counts (``zcount``), staged by the
+        caller (tables.stage_ion); by default they are uploaded and cached
+        with the grid's host tables."""
         self.dev = dev
         plan = dev.plan
         nv, ng = dev.nv, dev.ng
@@ -251,8 +256,9 @@ class IonRows:
         self.factors = H["factors"]
         kmax = max(plan.ks)
         d = dev.Pv.device
-        self.ktab = _device_table(H, "flat", d)
-        self.koff = _device_table(H, "koff", d)
+        dt = device_tables
+        self.ktab = dt["flat"] if dt else _device_table(H, "flat", d)
+        self.koff = dt["koff"] if dt else _device_table(H, "koff", d)
         self.kbody = (nv - 1) * ng
         self.nz = dict(H["nz"])
         max_z = max(self.nz.values())
@@ -288,17 +294,20 @@ class IonRows:
         self.fused = kind == "fused"
         self.ktab_t = self.koff_t = None
         if kind == "cells":  # cell-minor copy of u, ell, C and L for coalesced per-cell reads
-            self.ktab_t = _device_table(H, "flat_t", d)
-            self.koff_t = _device_table(H, "koff_t", d)
+            self.ktab_t = dt["flat_t"] if dt else _device_table(H, "flat_t", d)
+            self.koff_t = dt["koff_t"] if dt else _device_table(H, "koff_t", d)
         self.max_z = max_z
         self.body_w = fused_body_width(nv, ng) if self.fused else self.kbody
         self.kdim = {k: _round_up(self.body_w + self.nz[k], self.KCHUNK) for k in plan.ks}
         self.kmax_dim = max(self.kdim.values())
         self.has_z = max_z > 0
-        zc = np.zeros(kmax + 1, dtype=np.int32)
-        for k in plan.ks:
-            zc[k] = self.nz[k]
-        self.zcount = torch.as_tensor(zc, device=d)
+        if dt:
+            self.zcount = dt["zcount"]
+        else:
+            zc = np.zeros(kmax + 1, dtype=np.int32)
+            for k in plan.ks:
+                zc[k] = self.nz[k]
+            self.zcount = torch.as_tensor(zc, device=d)
 
     def column_positions(self, k: int) -> np.ndarray:
         """Residue position of every column of the row [X | Z] of multipole k."""

@@ -28,7 +28,7 @@ from .device import as_device, resident
 from .plan import TablePlan, make_plan
 from .yk import yk_partial_matrices
 
-__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "HostPackedTables", "PackedShipper", "packed_offsets", "upload_ion", "upload_values", "slater_rk_tables",
+__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "HostPackedTables", "PackedShipper", "packed_offsets", "upload_ion", "stage_ion", "upload_values", "slater_rk_tables",
            "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE",
            "Fp64Recompute", "fp64_tables_to_host"]
 
@@ -85,6 +85,79 @@ def upload_ion(ion, k_max: int | None = None, plan: TablePlan | None = None, str
     return IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=r, w=w, mo=mo, mi=mi, Pv=Pv, Qv=Qv,
                      pairs=pairs, row_pair=row_pair, row_k=row_k,
                      extra={"r_host": np.asarray(bsp["gr"], dtype=np.float64).reshape(-1)})
+
+
+_STAGE_ALIGN = 256
+
+
+def stage_ion(ion, plan: TablePlan, stream, pinned=None, factor_tables: dict | None = None):
+    """Device inputs of one ion in ONE device allocation and ONE host-to-device
+    copy, for callers that prepare many ions with new grids (a serving
+    planner): the grid, weights, partial matrices, B-spline values,
+    coefficients and plan arrays (and, with ``factor_tables`` =
+    split.host_tables(...), the split engine's factor tables and Z counts)
+    are packed into the pinned host buffer ``pinned`` (a uint8 CPU tensor;
+    grown and returned when too small), copied on ``stream``, and the
+    orbital values (K1) are evaluated into the same allocation.
+
+    Returns (IonDevice, device factor tables or None, pinned buffer).  The
+    pinned buffer may be reused once ``stream`` has passed the copy.  Every
+    array equals what ``upload_ion`` gives."""
+    L = _native.require_device()
+    bsp = ion.bsp
+    nv, ng = bsp["gr"].shape
+    n = nv * ng
+    mo_h, mi_h = yk_partial_matrices(ng)
+    parts = [("r", np.asarray(bsp["gr"], dtype=np.float64).reshape(-1)),
+             ("w", np.asarray(bsp["grw"], dtype=np.float64).reshape(-1)),
+             ("mo", np.asarray(mo_h, dtype=np.float64)), ("mi", np.asarray(mi_h, dtype=np.float64)),
+             ("bp", np.asarray(bsp["bsp_p"], dtype=np.float64)), ("bq", np.asarray(bsp["bsp_q"], dtype=np.float64)),
+             ("cp", np.asarray(ion.P, dtype=np.float64)), ("cq", np.asarray(ion.Q, dtype=np.float64)),
+             ("pairs", plan.pairs.reshape(-1).astype(np.int64, copy=False)),
+             ("row_pair", plan.row_pair.astype(np.int64, copy=False)),
+             ("row_k", plan.row_k.astype(np.int32))]
+    if factor_tables is not None:
+        H = factor_tables
+        zc = np.zeros(max(plan.ks) + 1, dtype=np.int32)
+        for k in plan.ks:
+            zc[k] = H["nz"][k]
+        parts += [("flat", H["flat"]), ("koff", H["koff"]), ("flat_t", H["flat_t"]), ("koff_t", H["koff_t"]),
+                  ("zcount", zc)]
+    offs, pos = [], 0
+    for _, a in parts:
+        offs.append(pos)
+        pos += -(-a.nbytes // _STAGE_ALIGN) * _STAGE_ALIGN
+    n_in = pos
+    n_orb = int(ion.P.shape[0])
+    out_off = pos
+    pos += 2 * n_orb * n * 8
+    if pinned is None or pinned.numel() < n_in:
+        pinned = torch.empty(max(n_in, 1 << 20), dtype=torch.uint8, pin_memory=True)
+    hb = pinned.numpy()
+    for (_, a), o in zip(parts, offs):
+        hb[o:o + a.nbytes].view(a.dtype)[:] = a.reshape(-1)
+    s = stream if stream is not None else torch.cuda.current_stream()
+    with torch.cuda.stream(s):
+        buf = torch.empty(pos, dtype=torch.uint8, device=torch.device("cuda", torch.cuda.current_device()))
+        buf[:n_in].copy_(pinned[:n_in], non_blocking=True)
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.int64): torch.int64, np.dtype(np.int32): torch.int32}
+    v = {name: buf[o:o + a.nbytes].view(tdt[a.dtype]).view(a.shape)
+         for (name, a), o in zip(parts, offs)}
+    Pv = buf[out_off:out_off + n_orb * n * 8].view(torch.float64).view(n_orb, n)
+    Qv = buf[out_off + n_orb * n * 8:pos].view(torch.float64).view(n_orb, n)
+    h = _native.stream_handle(s)
+    cp, cq = v["cp"], v["cq"]
+    _native.check(L.rkb_eval_orbitals(cp.data_ptr(), cp.shape[1], n_orb, v["bp"].data_ptr(), nv, ng, bsp["ksp"],
+                                      bsp["nsp"], Pv.data_ptr(), n, h), "rkb_eval_orbitals(P)")
+    _native.check(L.rkb_eval_orbitals(cq.data_ptr(), cq.shape[1], n_orb, v["bq"].data_ptr(), nv, ng, bsp["ksq"],
+                                      bsp["nsq"], Qv.data_ptr(), n, h), "rkb_eval_orbitals(Q)")
+    dev = IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=v["r"], w=v["w"], mo=v["mo"], mi=v["mi"], Pv=Pv, Qv=Qv,
+                    pairs=v["pairs"], row_pair=v["row_pair"], row_k=v["row_k"],
+                    extra={"r_host": parts[0][1]})
+    tables = None
+    if factor_tables is not None:
+        tables = {k: v[k] for k in ("flat", "koff", "flat_t", "koff_t", "zcount")}
+    return dev, tables, pinned
 
 
 def _plan_arrays(plan: TablePlan):

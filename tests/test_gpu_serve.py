@@ -7,6 +7,7 @@ every request must be identical in all runs, since no request's work depends
 on another's. The report carries p50/p99 latency, throughput and the group
 sizes.
 """
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -144,3 +145,46 @@ def test_served_cancelling_ion_is_within_the_gate(sink, max_group):
     # the cancelling table itself came from the FP64 engine
     assert float((target.sink.tables[7] - plain.table(7)).abs().max()) <= 1e-14 * float(plain.table(7).abs().max())
     server.close()
+
+
+@pytest.mark.parametrize("name", ["ytterbium_scaleup", "neon_small"])
+def test_staged_inputs_equal_uploaded_ones(name):
+    """tables.stage_ion (one pinned buffer, one copy, orbitals evaluated into
+    the same allocation) gives every array upload_ion gives, and the staged
+    factor tables equal the cached device copies; a batch over staged inputs
+    gives the same tables as over uploaded ones."""
+    from atomx_b200 import workloads as W
+    from atomx_b200.batch import SplitBatch
+    from atomx_b200.plan import make_plan
+    from atomx_b200.split import IonRows, host_tables
+    from atomx_b200.tables import stage_ion, upload_ion
+    spec = getattr(W, name)()
+    ion = W.build_ion(spec)
+    plan = make_plan(ion.kappa, spec.k_max)
+    H = host_tables(np.asarray(ion.bsp["gr"], dtype=np.float64).reshape(-1), ion.bsp["gr"].shape[1], plan.ks)
+    s = torch.cuda.Stream()
+    staged, dtab, pinned = stage_ion(ion, plan, s, None, H)
+    s.synchronize()
+    ref = upload_ion(ion, k_max=spec.k_max, plan=plan)
+    torch.cuda.synchronize()
+    for f in ("r", "w", "mo", "mi", "Pv", "Qv", "pairs", "row_pair", "row_k"):
+        a, b = getattr(staged, f), getattr(ref, f)
+        assert a.dtype == b.dtype and torch.equal(a.reshape(-1), b.reshape(-1)), f
+    rows_s, rows_r = IonRows(staged, device_tables=dtab), IonRows(ref)
+    for f in ("ktab", "koff", "zcount"):
+        assert torch.equal(getattr(rows_s, f), getattr(rows_r, f)), f
+    assert rows_s.kind == rows_r.kind
+    if rows_r.ktab_t is not None:
+        assert torch.equal(rows_s.ktab_t, rows_r.ktab_t) and torch.equal(rows_s.koff_t, rows_r.koff_t)
+    a = SplitBatch([staged], ion_rows=[rows_s])
+    b = SplitBatch([ref], ion_rows=[rows_r])
+    a.step()
+    b.step()
+    a.check_status()
+    b.check_status()
+    assert torch.equal(a.out, b.out)
+    # a second, smaller ion reuses the grown pinned buffer
+    small = W.build_ion(W.neon_small())
+    p2 = make_plan(small.kappa, 2)
+    _, _, pinned2 = stage_ion(small, p2, s, pinned, None)
+    assert pinned2 is pinned
