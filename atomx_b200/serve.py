@@ -508,3 +508,44 @@ class SlaterServer:
         for slot in self.slots:  # the workspaces go back to the device
             slot.ws.chunks = []
         torch.cuda.empty_cache()
+
+
+def main(argv=None) -> int:
+    """Serve the seeded mixed-ion request stream once and print the report
+    as one JSON line: ``python -m atomx_b200.serve [--requests N]
+    [--precision split|fp64] [--offline]``.  ``--offline`` plans every
+    request first and hands them all to the server at once (the device's
+    capacity on the mix); otherwise they arrive in real time."""
+    import argparse
+    import json
+
+    from . import workloads as W
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--requests", type=int, default=300)
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"])
+    ap.add_argument("--slots", type=int, default=2)
+    ap.add_argument("--max-group", type=int, default=16)
+    ap.add_argument("--offline", action="store_true")
+    args = ap.parse_args(argv)
+    stream = W.serving_requests(n_requests=args.requests)
+    reqs = [Request(rid=i, ion=W.build_ion(spec), k_max=spec.k_max, arrival=t) for i, (t, spec) in enumerate(stream)]
+    server = SlaterServer(precision=args.precision, max_inflight=args.slots, max_group=args.max_group)
+    try:
+        if args.offline:
+            for r in reqs:
+                server._plan(r)
+            server._plan = lambda r: r  # planned already
+        torch.cuda.synchronize()
+        rep = server.serve(reqs, realtime=not args.offline)
+        torch.cuda.synchronize()
+    finally:
+        server.close()
+    out = rep.summary()
+    out.update(offline=args.offline, p99_bound_ms=P99_BOUND_MS,
+               errors=[repr(r.error) for r in reqs if r.error is not None][:3])
+    print(json.dumps(out))
+    return 0 if not out["errors"] else 1
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
