@@ -70,21 +70,31 @@ int sm_count() {
 
 // ------------------------------------------------------------ Y^k kernels
 // Density source for a row: either an explicit row or a pair of orbitals.
+// ``row(q)`` resolves a row's source pointers once; ``at(i)`` reads node i.
 struct RhoRows {
     const double *rho;
     long ld;
-    __device__ __forceinline__ double at(long q, long i) const { return rho[q * ld + i]; }
+    struct Row {
+        const double *__restrict__ rho;
+        __device__ __forceinline__ double at(long i) const { return __ldg(rho + i); }
+    };
+    __device__ __forceinline__ Row row(long q) const { return Row{rho + q * ld}; }
 };
 struct RhoPairs {
     const double *P, *Q;
     long orb_ld;
     const long *pairs, *row_pair;
-    __device__ __forceinline__ double at(long q, long i) const {
-        long p = row_pair[q];
-        long a = pairs[2 * p], c = pairs[2 * p + 1];
+    struct Row {
+        const double *__restrict__ pa, *__restrict__ pc, *__restrict__ qa, *__restrict__ qc;
         // rho = P_a P_c + Q_a Q_c (atomx slater_yk.py:193), each product rounded
-        return __dadd_rn(__dmul_rn(P[a * orb_ld + i], P[c * orb_ld + i]),
-                         __dmul_rn(Q[a * orb_ld + i], Q[c * orb_ld + i]));
+        __device__ __forceinline__ double at(long i) const {
+            return __dadd_rn(__dmul_rn(__ldg(pa + i), __ldg(pc + i)), __dmul_rn(__ldg(qa + i), __ldg(qc + i)));
+        }
+    };
+    __device__ __forceinline__ Row row(long q) const {
+        const long p = row_pair[q];
+        const long a = pairs[2 * p], c = pairs[2 * p + 1];
+        return Row{P + a * orb_ld, P + c * orb_ld, Q + a * orb_ld, Q + c * orb_ld};
     }
 };
 
@@ -108,6 +118,7 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
     if (q >= nrows) return;
     const int k = row_k ? row_k[q] : k_all;
     const int nchunks = (nv + 31) >> 5;
+    const auto sr = src.row(q);  // the row's source pointers, resolved once
 
     // ---- outward pass: A_m carried left to right
     double carry = 0.0;
@@ -121,10 +132,10 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
             for (int j = 0; j < NGMAX; ++j) {
                 if (j < ng) {
                     long i = (long)m * ng + j;
-                    double rho = src.at(q, i);
-                    double g = __dmul_rn(w[i], rho);
+                    double rho = sr.at(i);
+                    double g = __dmul_rn(__ldg(w + i), rho);
                     if (gout) gout[q * yk_ld + i] = g;
-                    h[j] = __dmul_rn(g, int_pow(r[i], k));
+                    h[j] = __dmul_rn(g, int_pow(__ldg(r + i), k));
                     cell = __dadd_rn(cell, h[j]);
                 }
             }
@@ -152,15 +163,17 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
     for (int c = 0; c < nchunks; ++c) {
         const int m = nv - 1 - ((c << 5) + lane);
         const bool live = m >= 0;
-        double e[NGMAX];
+        double e[NGMAX], rin[NGMAX];  // r^-(k+1) of this cell's nodes (a division each), kept for Y
         double cell = 0.0;
         if (live) {
 #pragma unroll
             for (int j = 0; j < NGMAX; ++j) {
                 if (j < ng) {
                     long i = (long)m * ng + j;
-                    double g = __dmul_rn(w[i], src.at(q, i));
-                    e[j] = __dmul_rn(g, int_pow(r[i], -(k + 1)));
+                    double g = __dmul_rn(__ldg(w + i), sr.at(i));
+                    const double ri = __ldg(r + i);
+                    rin[j] = int_pow(ri, -(k + 1));
+                    e[j] = __dmul_rn(g, rin[j]);
                     cell = __dadd_rn(cell, e[j]);
                 }
             }
@@ -178,9 +191,8 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
                     for (int j = 0; j < NGMAX; ++j)
                         if (j < ng) s = __dadd_rn(s, __dmul_rn(e[j], __ldg(&mi[i * ng + j])));
                     long idx = (long)m * ng + i;
-                    double ri = r[idx];
-                    yk[q * yk_ld + idx] = __dadd_rn(__dmul_rn(int_pow(ri, -(k + 1)), iout[idx]),
-                                                    __dmul_rn(int_pow(ri, k), s));
+                    yk[q * yk_ld + idx] =
+                        __dadd_rn(__dmul_rn(rin[i], iout[idx]), __dmul_rn(int_pow(__ldg(r + idx), k), s));
                 }
             }
         }
