@@ -101,6 +101,16 @@ struct RhoPairs {
 // One warp per row; NG is the compile-time node count (0 = runtime ng <= RKB_MAX_NG).
 // `gout` (optional) receives g = w*rho for the row (table engine), and columns
 // n..ld-1 of both outputs are zero-filled.
+//
+// Each pass walks the row in chunks of 32 cells.  The element-wise work of a
+// chunk (rho, g, the powers of r, the output Y) runs with consecutive lanes on
+// consecutive nodes, so every global load and store is coalesced; the
+// per-cell terms meet the cell-owning lane through a per-warp buffer of
+// 32 cells x GS doubles (GS = ng | 1: odd stride, no bank conflicts), and the
+// cell sums, the warp scan and the partial-matrix sums run as before, lane l
+// owning one cell.  I_out waits in the output row between the passes.  Every
+// product and sum is the one the cell-per-lane form evaluates, in the same
+// order, so the rows are bit-identical to it.
 template <int NG, class Src>
 __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__restrict__ row_k, int k_all, long nrows,
                                                       const double *__restrict__ r, const double *__restrict__ w,
@@ -108,22 +118,38 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
                                                       const double *__restrict__ mi, double *__restrict__ yk,
                                                       long yk_ld, double *__restrict__ gout) {
     constexpr int NGMAX = NG > 0 ? NG : RKB_MAX_NG;
+    constexpr int GSMAX = NGMAX | 1;
     const int ng = NG > 0 ? NG : ng_rt;
-    extern __shared__ double smem_iout[];
+    const int gs = NG > 0 ? (NG | 1) : (ng_rt | 1);
+    extern __shared__ double smem_chunk[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const long n = (long)nv * ng;
-    double *iout = smem_iout + (long)wib * n;
+    double *cbuf = smem_chunk + (long)wib * (32 * GSMAX);  // [32][gs]: one chunk's per-node terms
     const long q = (long)blockIdx.x * (blockDim.x >> 5) + wib;
     if (q >= nrows) return;
     const int k = row_k ? row_k[q] : k_all;
     const int nchunks = (nv + 31) >> 5;
     const auto sr = src.row(q);  // the row's source pointers, resolved once
+    double *yrow = yk + q * yk_ld;
+    double *grow_ = gout ? gout + q * yk_ld : nullptr;
 
-    // ---- outward pass: A_m carried left to right
+    // ---- outward pass: A_m carried left to right; lane l owns cell 32c + l
     double carry = 0.0;
     for (int c = 0; c < nchunks; ++c) {
-        const int m = (c << 5) + lane;
+        const int m0 = c << 5;
+        const int ncell = min(32, nv - m0);
+        const long e0 = (long)m0 * ng, ne = (long)ncell * ng;
+        // element-wise: h = (w rho) r^k, consecutive lanes on consecutive nodes
+        for (long t = lane; t < ne; t += 32) {
+            const long i = e0 + t;
+            const double g = __dmul_rn(__ldg(w + i), sr.at(i));
+            if (grow_) grow_[i] = g;
+            const int cl = (int)(t / ng), node = (int)(t - (long)cl * ng);
+            cbuf[cl * gs + node] = __dmul_rn(g, int_pow(__ldg(r + i), k));
+        }
+        __syncwarp();
+        const int m = m0 + lane;
         const bool live = m < nv;
         double h[NGMAX];
         double cell = 0.0;
@@ -131,11 +157,7 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
 #pragma unroll
             for (int j = 0; j < NGMAX; ++j) {
                 if (j < ng) {
-                    long i = (long)m * ng + j;
-                    double rho = sr.at(i);
-                    double g = __dmul_rn(__ldg(w + i), rho);
-                    if (gout) gout[q * yk_ld + i] = g;
-                    h[j] = __dmul_rn(g, int_pow(__ldg(r + i), k));
+                    h[j] = cbuf[lane * gs + j];
                     cell = __dadd_rn(cell, h[j]);
                 }
             }
@@ -152,28 +174,49 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
 #pragma unroll
                     for (int j = 0; j < NGMAX; ++j)
                         if (j < ng) s = __dadd_rn(s, __dmul_rn(h[j], __ldg(&mo[i * ng + j])));
-                    iout[(long)m * ng + i] = s;
+                    cbuf[lane * gs + i] = s;  // own slots only: h is in registers
                 }
             }
         }
+        __syncwarp();
+        // I_out parked in the output row (coalesced); the inward pass reads it
+        // back and overwrites it with Y
+        for (long t = lane; t < ne; t += 32) {
+            const int cl = (int)(t / ng), node = (int)(t - (long)cl * ng);
+            yrow[e0 + t] = cbuf[cl * gs + node];
+        }
+        __syncwarp();  // cbuf is rewritten by the next chunk
     }
-    __syncwarp();
     // ---- inward pass: B_m carried right to left; lane l owns cell (end - l)
     carry = 0.0;
     for (int c = 0; c < nchunks; ++c) {
-        const int m = nv - 1 - ((c << 5) + lane);
+        const int mhi = nv - 1 - (c << 5);             // cell of lane 0
+        const int mlo = max(0, mhi - 31);               // lowest cell of the chunk
+        const long e0 = (long)mlo * ng, ne = (long)(mhi - mlo + 1) * ng;
+        // element-wise: r^-(k+1) (kept in registers for Y) and e = (w rho) r^-(k+1)
+        double rin[NGMAX];
+#pragma unroll
+        for (int u = 0; u < NGMAX; ++u) {
+            const long t = lane + 32L * u;
+            if (u < ng && t < ne) {
+                const long i = e0 + t;
+                const double g = __dmul_rn(__ldg(w + i), sr.at(i));
+                rin[u] = int_pow(__ldg(r + i), -(k + 1));
+                const int cl = (int)(t / ng), node = (int)(t - (long)cl * ng);
+                cbuf[cl * gs + node] = __dmul_rn(g, rin[u]);
+            }
+        }
+        __syncwarp();
+        const int m = mhi - lane;
         const bool live = m >= 0;
-        double e[NGMAX], rin[NGMAX];  // r^-(k+1) of this cell's nodes (a division each), kept for Y
+        const int cl_m = m - mlo;  // this lane's cell in the chunk buffer
+        double e[NGMAX];
         double cell = 0.0;
         if (live) {
 #pragma unroll
             for (int j = 0; j < NGMAX; ++j) {
                 if (j < ng) {
-                    long i = (long)m * ng + j;
-                    double g = __dmul_rn(__ldg(w + i), sr.at(i));
-                    const double ri = __ldg(r + i);
-                    rin[j] = int_pow(ri, -(k + 1));
-                    e[j] = __dmul_rn(g, rin[j]);
+                    e[j] = cbuf[cl_m * gs + j];
                     cell = __dadd_rn(cell, e[j]);
                 }
             }
@@ -182,6 +225,8 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
         double excl = __shfl_up_sync(0xffffffffu, incl, 1);
         double base = lane == 0 ? carry : __dadd_rn(carry, excl);
         carry = __dadd_rn(carry, __shfl_sync(0xffffffffu, incl, 31));
+        // I_in of this lane's cell back into its buffer slots (each lane reads
+        // and writes only its own cell's slots)
         if (live) {
 #pragma unroll
             for (int i = 0; i < NGMAX; ++i) {
@@ -190,17 +235,27 @@ __global__ void __launch_bounds__(128) yk_rows_kernel(Src src, const int *__rest
 #pragma unroll
                     for (int j = 0; j < NGMAX; ++j)
                         if (j < ng) s = __dadd_rn(s, __dmul_rn(e[j], __ldg(&mi[i * ng + j])));
-                    long idx = (long)m * ng + i;
-                    yk[q * yk_ld + idx] =
-                        __dadd_rn(__dmul_rn(rin[i], iout[idx]), __dmul_rn(int_pow(__ldg(r + idx), k), s));
+                    cbuf[cl_m * gs + i] = s;
                 }
             }
         }
+        __syncwarp();
+        // element-wise: Y = r^-(k+1) I_out + r^k I_in, coalesced
+#pragma unroll
+        for (int u = 0; u < NGMAX; ++u) {
+            const long t = lane + 32L * u;
+            if (u < ng && t < ne) {
+                const long i = e0 + t;
+                const int cl = (int)(t / ng), node = (int)(t - (long)cl * ng);
+                yrow[i] = __dadd_rn(__dmul_rn(rin[u], yrow[i]), __dmul_rn(int_pow(__ldg(r + i), k), cbuf[cl * gs + node]));
+            }
+        }
+        __syncwarp();  // cbuf is rewritten by the next chunk
     }
     // zero padding columns
     for (long i = n + lane; i < yk_ld; i += 32) {
-        yk[q * yk_ld + i] = 0.0;
-        if (gout) gout[q * yk_ld + i] = 0.0;
+        yrow[i] = 0.0;
+        if (grow_) grow_[i] = 0.0;
     }
 }
 
@@ -209,12 +264,10 @@ static int launch_yk(Src src, const int *d_row_k, int k_all, long nrows, const d
                      int ng, const double *d_mo, const double *d_mi, double *d_yk, long yk_ld, double *d_g,
                      cudaStream_t st) {
     const int warps = 4;
-    long n = (long)nv * ng;
-    size_t smem = (size_t)warps * n * sizeof(double);
-    if (smem > 200 * 1024) {
-        set_error("grid of %ld nodes exceeds the Y^k kernel's shared-memory limit", n);
-        return RKB_EINVAL;
-    }
+    // the kernel's GSMAX: ng | 1 for the compiled node counts below, RKB_MAX_NG | 1 otherwise
+    const bool compiled = (ng >= 2 && ng <= 13) || ng == 16 || ng == 17;
+    const int gsmax = compiled ? (ng | 1) : (RKB_MAX_NG | 1);
+    const size_t smem = (size_t)warps * 32 * gsmax * sizeof(double);  // one chunk buffer per warp, any grid length
     dim3 grid((unsigned)ceil_div(nrows, warps)), block(32 * warps);
 #define RKB_YK_CASE(NGV)                                                                                  \
     case NGV: {                                                                                           \
@@ -375,11 +428,19 @@ int rkb_device_supported(void) {
     return major == 10 ? 1 : 0;
 }
 
+// The output rows hold I_out between the kernel's two passes, so they must not
+// overlap the density rows the second pass reads again.
+static bool overlaps(const double *a, long a_rows, long a_ld, const double *b, long b_rows, long b_ld, long n) {
+    const double *a1 = a + (a_rows - 1) * a_ld + n, *b1 = b + (b_rows - 1) * b_ld + n;
+    return a < b1 && b < a1;
+}
+
 int rkb_yk_flat(const double *d_rho, const double *d_r, const double *d_w, long n, int k, int nv, int ng,
                 const double *d_mo, const double *d_mi, double *d_yk, void *stream) {
     int st = check_grid(nv, ng, n);
     if (st) return st;
     RKB_CHECK_ARG(k >= 0 && k <= 64, "multipole rank must be an integer in [0, 64] (got %d)", k);
+    RKB_CHECK_ARG(!overlaps(d_rho, 1, n, d_yk, 1, n, n), "d_yk must not overlap d_rho");
     return launch_yk(RhoRows{d_rho, n}, nullptr, k, 1, d_r, d_w, nv, ng, d_mo, d_mi, d_yk, n, nullptr,
                      as_stream(stream));
 }
@@ -393,6 +454,7 @@ int rkb_yk_rows(const double *d_rho, long rho_ld, const int *d_row_k, long nrows
     RKB_CHECK_ARG(nrows >= 0, "nrows must be >= 0");
     RKB_CHECK_ARG(rho_ld >= n && yk_ld >= n, "leading dimensions must be >= nv*ng");
     if (nrows == 0) return RKB_OK;
+    RKB_CHECK_ARG(!overlaps(d_rho, nrows, rho_ld, d_yk, nrows, yk_ld, n), "d_yk must not overlap d_rho");
     return launch_yk(RhoRows{d_rho, rho_ld}, d_row_k, 0, nrows, d_r, d_w, nv, ng, d_mo, d_mi, d_yk, yk_ld, nullptr,
                      as_stream(stream));
 }

@@ -54,7 +54,9 @@ int rkb_yk_flat(const double *d_rho, const double *d_r, const double *d_w, long 
 
 /* Batched rows: row q reads density d_rho + q*rho_ld, uses multipole
  * d_row_k[q] and writes d_yk + q*yk_ld.  Same rule as rkb_yk_flat
- * (atomx numerics/yk.py:157 compute_yk applied per row). */
+ * (atomx numerics/yk.py:157 compute_yk applied per row).  In both, the
+ * output must not overlap the density (RKB_EINVAL): the output rows hold
+ * the outward sums until the inward pass has read the density again. */
 int rkb_yk_rows(const double *d_rho, long rho_ld, const int *d_row_k, long nrows,
                 const double *d_r, const double *d_w, int nv, int ng,
                 const double *d_mo, const double *d_mi, double *d_yk, long yk_ld,
