@@ -434,15 +434,26 @@ class SlaterServer:
         groups, fp64 = [], 0
         self._t0 = time.perf_counter()
         now = self._now
+        # The loop sleeps until something changes: a plan or a group completes
+        # (their futures set `wake`) or the next request arrives.  Waking at a
+        # fixed short period instead would take the GIL thousands of times a
+        # second from the planners and launchers.
+        wake = threading.Event()
+
+        def notify(_fut):
+            wake.set()
 
         while todo or planning or ready or inflight:
+            wake.clear()
             t = now()
             # arrivals: (in real time, or all at once when not realtime)
             while todo and (not realtime or todo[0].arrival <= t):
                 r = todo.popleft()
                 if not realtime:
                     r.arrival = t
-                planning.append((r, self.pool.submit(self._plan, r)))
+                fut = self.pool.submit(self._plan, r)
+                fut.add_done_callback(notify)
+                planning.append((r, fut))
             # planned requests join the ready queue in arrival order
             still = []
             for r, fut in planning:
@@ -489,10 +500,17 @@ class SlaterServer:
                     r.admitted = ta
                 used += gfp
                 groups.append(len(group))
-                inflight.append((group, gfp, slot, self.launchers.submit(self._run_group, group, slot)))
+                fut = self.launchers.submit(self._run_group, group, slot)
+                fut.add_done_callback(notify)
+                inflight.append((group, gfp, slot, fut))
                 max_seen = max(max_seen, sum(len(g[0]) for g in inflight))
             if not admitted:
-                time.sleep(2e-4)
+                # until the next arrival at most (a future that completed
+                # since the clear() above has set the event already)
+                timeout = 0.05
+                if realtime and todo:
+                    timeout = min(timeout, max(0.0, todo[0].arrival - now()))
+                wake.wait(timeout)
         wall = now()
         done = [r for r in requests if r.error is None]
         stages = {k: [r.timing[k] for r in done if k in r.timing]
