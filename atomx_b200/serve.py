@@ -547,8 +547,11 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     stream = W.serving_requests(n_requests=args.requests)
     reqs = [Request(rid=i, ion=W.build_ion(spec), k_max=spec.k_max, arrival=t) for i, (t, spec) in enumerate(stream)]
+    warm = [Request(rid=-1 - i, ion=W.build_ion(spec), k_max=spec.k_max)
+            for i, (_, spec) in enumerate(W.serving_requests(seed=7, n_requests=8))]
     server = SlaterServer(precision=args.precision, max_inflight=args.slots, max_group=args.max_group)
     try:
+        server.serve(warm, realtime=False)  # another seed: warms kernels and pools, caches nothing measured
         if args.offline:
             for r in reqs:
                 server._plan(r)
