@@ -188,3 +188,15 @@ def test_staged_inputs_equal_uploaded_ones(name):
     p2 = make_plan(small.kappa, 2)
     _, _, pinned2 = stage_ion(small, p2, s, pinned, None)
     assert pinned2 is pinned
+
+
+def test_command_line_serves_the_stream(capsys):
+    """``python -m atomx_b200.serve``: a short run of the seeded stream
+    (after its warm-up requests) reports every request served."""
+    import json
+
+    from atomx_b200.serve import main
+    assert main(["--requests", "6", "--offline"]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["requests"] == 6 and out["errors"] == [] and out["offline"] is True
+    assert out["p99_ms"] >= out["p50_ms"] > 0 and out["throughput_entries_per_s"] > 0
