@@ -47,6 +47,7 @@ from other ions, so a request gives the same tables alone and in any group;
 """
 from __future__ import annotations
 
+import gc
 import threading
 import time
 from collections import deque
@@ -423,10 +424,29 @@ class SlaterServer:
             fp = nxt
         return group, fp
 
-    def serve(self, requests: list[Request], realtime: bool = True) -> ServeReport:
+    def serve(self, requests: list[Request], realtime: bool = True, pause_gc: bool = True) -> ServeReport:
         """Run the requests (sorted by arrival) to completion; return timings.
         ``realtime``: requests arrive at their arrival times; otherwise all
-        arrive at once and are planned before the first group starts."""
+        arrive at once and are planned before the first group starts.
+
+        ``pause_gc``: collect once before the clock starts, then keep
+        Python's cyclic garbage collector off while serving (its previous
+        state is restored on return).  A full collection walks every object
+        of the process while holding the GIL; in a process with a large heap
+        that is a pause of a large fraction of a second in which no request
+        is planned or launched.  Reference counting still frees the
+        requests' objects as they complete."""
+        was_enabled = gc.isenabled()
+        if pause_gc:
+            gc.collect()
+            gc.disable()
+        try:
+            return self._serve(requests, realtime)
+        finally:
+            if pause_gc and was_enabled:
+                gc.enable()
+
+    def _serve(self, requests: list[Request], realtime: bool) -> ServeReport:
         todo = deque(sorted(requests, key=lambda r: r.arrival))
         planning, ready, inflight, free_slots = [], deque(), [], list(self.slots)
         used = 0
