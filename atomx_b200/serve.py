@@ -137,6 +137,7 @@ class ServeReport:
     stages_ms: dict = field(default_factory=dict)   # stage -> per-request times (ms)
     group_sizes: list = field(default_factory=list)  # requests per admitted group
     fp64_tables: int = 0                              # split tables recomputed in FP64
+    tail: list = field(default_factory=list)          # timelines of the slowest 1 % of requests
 
     def summary(self) -> dict:
         lat = np.asarray(self.latencies_ms)
@@ -149,7 +150,8 @@ class ServeReport:
                 "queue_p99_ms": float(np.percentile(q, 99)), "precision": self.precision,
                 "max_inflight": self.max_inflight_seen, "groups": len(self.group_sizes),
                 "group_size_mean": float(np.mean(self.group_sizes)) if self.group_sizes else 0.0,
-                "group_size_max": int(max(self.group_sizes, default=0)), "fp64_tables": self.fp64_tables}
+                "group_size_max": int(max(self.group_sizes, default=0)), "fp64_tables": self.fp64_tables,
+                "tail": self.tail}
 
 
 def footprint_parts(ion, plan, precision: str, whole_tables: bool = False) -> tuple[int, int, int, int]:
@@ -535,10 +537,16 @@ class SlaterServer:
         done = [r for r in requests if r.error is None]
         stages = {k: [r.timing[k] for r in done if k in r.timing]
                   for k in ("plan_ms", "stage_ms", "launch_host_ms", "after_enqueue_ms")}
+        # where the slowest requests spent their time (server clock, ms)
+        slow = sorted(done, key=lambda r: r.latency, reverse=True)[:max(3, len(done) // 100)]
+        tail = [dict({"rid": r.rid, "arrival": 1e3 * r.arrival, "planned": 1e3 * (r.planned - r.arrival),
+                      "admitted": 1e3 * (r.admitted - r.arrival), "done": 1e3 * r.latency, "entries": r.entries},
+                     **{k: round(v, 2) for k, v in r.timing.items()}) for r in slow]
         return ServeReport(n=len(requests), wall_s=wall, entries=int(sum(r.entries for r in done)),
                            latencies_ms=[1e3 * r.latency for r in done],
                            queue_ms=[1e3 * (r.admitted - r.arrival) for r in done], precision=self.precision,
-                           max_inflight_seen=max_seen, stages_ms=stages, group_sizes=groups, fp64_tables=fp64)
+                           max_inflight_seen=max_seen, stages_ms=stages, group_sizes=groups, fp64_tables=fp64,
+                           tail=tail)
 
     def close(self):
         self.pool.shutdown(wait=True)
