@@ -12,7 +12,7 @@ import torch
 
 from . import _native
 
-__all__ = ["as_device", "resident", "to_host", "is_device_tensor", "device"]
+__all__ = ["as_device", "resident", "to_host", "is_device_tensor", "device", "wait_for"]
 
 _cache: OrderedDict = OrderedDict()
 _cache_lock = threading.Lock()
@@ -62,3 +62,14 @@ def resident(x, dtype=torch.float64) -> torch.Tensor:
 
 def to_host(t: torch.Tensor) -> np.ndarray:
     return t.detach().to("cpu").numpy()
+
+
+def wait_for(stream) -> None:
+    """Block the calling host thread until ``stream`` has run the work queued
+    on it so far, asleep in the driver rather than spinning: the wait goes
+    through an event created with the blocking-sync flag.  Threads that spin
+    while they wait use a core each; in a process with a CPU quota several of
+    them can use it up and get the whole process throttled."""
+    ev = torch.cuda.Event(blocking=True)
+    ev.record(stream)
+    ev.synchronize()

@@ -58,6 +58,7 @@ import numpy as np
 import torch
 
 from .batch import Fp64Batch, SplitBatch, Workspace
+from .device import wait_for
 from .plan import make_plan
 from .split import KDIM_MAX, IonRows, check_kdim, host_tables
 from .split_plan import bits_for_moduli, moduli_needed
@@ -302,7 +303,7 @@ class SlaterServer:
             dev, dtab, pinned = stage_ion(req.ion, req.plan, ps, getattr(self._tls, "pinned", None), H)
             rows = IonRows(dev, device_tables=dtab) if split else None
         self._tls.pinned = pinned
-        ps.synchronize()  # the launcher's stream reads them; the pinned buffer is free again
+        wait_for(ps)  # the launcher's stream reads them; the pinned buffer is free again
         if rows is not None:
             check_kdim(rows.kmax_dim)  # a grid the split engine does not take fails this request alone
         req.state["dev"], req.state["ion_rows"] = dev, rows
@@ -346,7 +347,7 @@ class SlaterServer:
                     r = group[i]
                     r.sink(k, b.table(i, k), r.plan.block_ranges_of_k(k), s)
                 if b.escalated:
-                    s.synchronize()
+                    wait_for(s)
             return len(b.escalated) if split else 0
         return complete
 
@@ -383,7 +384,9 @@ class SlaterServer:
                     complete = self._stream_one(group[0], slot)
                 else:
                     complete = self._batch(group, slot)
-                ev = torch.cuda.Event()
+                # the launcher sleeps until the group is done (a blocking-sync
+                # event: no core spent spinning, see device.wait_for)
+                ev = torch.cuda.Event(blocking=True)
                 ev.record(s)
                 t_enq = time.perf_counter()
                 ev.synchronize()
