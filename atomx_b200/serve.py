@@ -62,7 +62,7 @@ from .device import wait_for
 from .plan import make_plan
 from .split import KDIM_MAX, IonRows, check_kdim, host_tables
 from .split_plan import bits_for_moduli, moduli_needed
-from .tables import stage_ion, upload_ion
+from .tables import evaluate_staged, stage_ion, upload_ion
 
 __all__ = ["Request", "ServeReport", "SlaterServer", "ChecksumSink", "footprint_bytes", "footprint_parts",
            "P99_BOUND_MS", "SERVE_N_MOD", "SERVE_CORR_FLOOR", "GROUP_BYTES"]
@@ -289,8 +289,10 @@ class SlaterServer:
         staging stream, off the launch path (``tables.stage_ion``):
         coefficients, the basis and plan arrays and, for the split engine,
         the factor tables, in one device allocation and one copy from the
-        thread's pinned buffer; then the orbital values (K1) and the split
-        engine's row side.  A new radial grid would otherwise make these a
+        thread's pinned buffer, and the split engine's row side.  The
+        orbital values (K1) are evaluated later, on the group's stream: a
+        kernel on the staging stream would wait for SMs behind a running
+        contraction, and the planners with it.  A new radial grid would otherwise make these a
         dozen synchronous copies on the launch path.  They are small beside
         the tables (orbital values: 16 bytes per spinor and grid node)."""
         ps = self._planner_stream()
@@ -300,7 +302,8 @@ class SlaterServer:
             H = host_tables(np.asarray(req.ion.bsp["gr"], dtype=np.float64).reshape(-1),
                             req.ion.bsp["gr"].shape[1], req.plan.ks)
         with torch.cuda.device(self.device), torch.cuda.stream(ps):
-            dev, dtab, pinned = stage_ion(req.ion, req.plan, ps, getattr(self._tls, "pinned", None), H)
+            dev, dtab, pinned = stage_ion(req.ion, req.plan, ps, getattr(self._tls, "pinned", None), H,
+                                          evaluate=False)
             rows = IonRows(dev, device_tables=dtab) if split else None
         self._tls.pinned = pinned
         wait_for(ps)  # the launcher's stream reads them; the pinned buffer is free again
@@ -311,7 +314,10 @@ class SlaterServer:
     @staticmethod
     def _dev(req: Request, stream):
         dev = req.state.get("dev")
-        return dev if dev is not None else upload_ion(req.ion, k_max=req.k_max, plan=req.plan, stream=stream)
+        if dev is None:
+            return upload_ion(req.ion, k_max=req.k_max, plan=req.plan, stream=stream)
+        evaluate_staged(dev, stream)  # K1 on the group's stream, ahead of its rows
+        return dev
 
     def _batch(self, group: list, slot: _Slot):
         """One batch over the group's ions on the slot's stream; every table

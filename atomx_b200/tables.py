@@ -28,7 +28,7 @@ from .device import as_device, resident
 from .plan import TablePlan, make_plan
 from .yk import yk_partial_matrices
 
-__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "HostPackedTables", "PackedShipper", "packed_offsets", "upload_ion", "stage_ion", "upload_values", "slater_rk_tables",
+__all__ = ["IonDevice", "RkTables", "RkStream", "HostTableSink", "HostPackedTables", "PackedShipper", "packed_offsets", "upload_ion", "stage_ion", "evaluate_staged", "upload_values", "slater_rk_tables",
            "slater_rk_tables_from_values", "tables_for", "stream_tables", "iter_blocks", "tile_tasks", "TILE",
            "Fp64Recompute", "fp64_tables_to_host"]
 
@@ -90,7 +90,24 @@ def upload_ion(ion, k_max: int | None = None, plan: TablePlan | None = None, str
 _STAGE_ALIGN = 256
 
 
-def stage_ion(ion, plan: TablePlan, stream, pinned=None, factor_tables: dict | None = None):
+def evaluate_staged(dev: IonDevice, stream) -> None:
+    """Evaluate the orbital values (K1) of an ion staged with
+    ``stage_ion(..., evaluate=False)`` on ``stream`` (once; later calls do
+    nothing)."""
+    pending = dev.extra.pop("pending_eval", None)
+    if pending is None:
+        return
+    L = _native.require_device()
+    cp, cq, bp, bq, ksp, nsp, ksq, nsq = pending
+    h = _native.stream_handle(stream)
+    n_orb = dev.Pv.shape[0]
+    _native.check(L.rkb_eval_orbitals(cp.data_ptr(), cp.shape[1], n_orb, bp.data_ptr(), dev.nv, dev.ng, ksp, nsp,
+                                      dev.Pv.data_ptr(), dev.n, h), "rkb_eval_orbitals(P)")
+    _native.check(L.rkb_eval_orbitals(cq.data_ptr(), cq.shape[1], n_orb, bq.data_ptr(), dev.nv, dev.ng, ksq, nsq,
+                                      dev.Qv.data_ptr(), dev.n, h), "rkb_eval_orbitals(Q)")
+
+
+def stage_ion(ion, plan: TablePlan, stream, pinned=None, factor_tables: dict | None = None, evaluate: bool = True):
     """Device inputs of one ion in ONE device allocation and ONE host-to-device
     copy, for callers that prepare many ions with new grids (a serving
     planner): the grid, weights, partial matrices, B-spline values,
@@ -98,12 +115,14 @@ def stage_ion(ion, plan: TablePlan, stream, pinned=None, factor_tables: dict | N
     split.host_tables(...), the split engine's factor tables and Z counts)
     are packed into the pinned host buffer ``pinned`` (a uint8 CPU tensor;
     grown and returned when too small), copied on ``stream``, and the
-    orbital values (K1) are evaluated into the same allocation.
+    orbital values (K1) are evaluated into the same allocation.  With
+    ``evaluate=False`` only the copy is queued (copy engines, no SM time)
+    and ``evaluate_staged`` runs K1 later, on the stream that uses the ion.
 
     Returns (IonDevice, device factor tables or None, pinned buffer).  The
     pinned buffer may be reused once ``stream`` has passed the copy.  Every
     array equals what ``upload_ion`` gives."""
-    L = _native.require_device()
+    _native.require_device()
     bsp = ion.bsp
     nv, ng = bsp["gr"].shape
     n = nv * ng
@@ -145,15 +164,13 @@ def stage_ion(ion, plan: TablePlan, stream, pinned=None, factor_tables: dict | N
          for (name, a), o in zip(parts, offs)}
     Pv = buf[out_off:out_off + n_orb * n * 8].view(torch.float64).view(n_orb, n)
     Qv = buf[out_off + n_orb * n * 8:pos].view(torch.float64).view(n_orb, n)
-    h = _native.stream_handle(s)
-    cp, cq = v["cp"], v["cq"]
-    _native.check(L.rkb_eval_orbitals(cp.data_ptr(), cp.shape[1], n_orb, v["bp"].data_ptr(), nv, ng, bsp["ksp"],
-                                      bsp["nsp"], Pv.data_ptr(), n, h), "rkb_eval_orbitals(P)")
-    _native.check(L.rkb_eval_orbitals(cq.data_ptr(), cq.shape[1], n_orb, v["bq"].data_ptr(), nv, ng, bsp["ksq"],
-                                      bsp["nsq"], Qv.data_ptr(), n, h), "rkb_eval_orbitals(Q)")
     dev = IonDevice(plan=plan, nv=nv, ng=ng, n=n, r=v["r"], w=v["w"], mo=v["mo"], mi=v["mi"], Pv=Pv, Qv=Qv,
                     pairs=v["pairs"], row_pair=v["row_pair"], row_k=v["row_k"],
-                    extra={"r_host": parts[0][1]})
+                    extra={"r_host": parts[0][1],
+                           "pending_eval": (v["cp"], v["cq"], v["bp"], v["bq"], bsp["ksp"], bsp["nsp"], bsp["ksq"],
+                                            bsp["nsq"])})
+    if evaluate:
+        evaluate_staged(dev, s)
     tables = None
     if factor_tables is not None:
         tables = {k: v[k] for k in ("flat", "koff", "flat_t", "koff_t", "zcount")}
