@@ -554,42 +554,45 @@ def e2e_leg(ion, engine, args, world, k_max):
 
 def serve_leg(args) -> dict:
     """The seeded Poisson request stream (rate 200/s) served by the
-    continuous-batching loop, split engine and plain FP64 engine in turn."""
-    from concurrent.futures import ThreadPoolExecutor
+    continuous-batching loop, split engine and plain FP64 engine in turn.
+
+    Each engine's server runs in a process of its own, as a server would
+    (``python -m atomx_b200.serve``, on this GPU, while this process waits):
+    it warms up on eight requests of another seed, then serves the stream in
+    real time and prints its report.  Served inside this process instead,
+    after the legs above, some runs stalled for a large fraction of a second
+    with the same code."""
+    import subprocess
 
     from atomx_b200 import workloads as W
-    from atomx_b200.serve import Request, SlaterServer
-    stream = W.serving_requests(n_requests=args.serve)
-    warm_specs = [spec for _, spec in W.serving_requests(seed=7, n_requests=8)]
-    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
-        ions = list(ex.map(lambda ts: W.build_ion(ts[1]), stream))  # client-side data, not timed
-        warm = list(zip(warm_specs, ex.map(W.build_ion, warm_specs)))
     from atomx_b200.serve import P99_BOUND_MS
+    stream = W.serving_requests(n_requests=args.serve)
     out = {"requests": len(stream), "rate_per_s": 200.0, "arrival_span_s": stream[-1][0],
            "sink": "device: per-(k, row) sums of every multipole table",
            "p99_bound_ms": P99_BOUND_MS,
            "note": "latency = last table delivered - arrival (server clock), realtime Poisson arrivals; "
                    "requests ready together run as one group (one batched contraction launch) in one of "
-                   f"{args.serve_slots} stream slots"}
+                   f"{args.serve_slots} stream slots; each engine's server in its own process "
+                   "(python -m atomx_b200.serve), warmed up on 8 requests of another seed"}
+    torch_sync()
+    import torch
+    torch.cuda.empty_cache()  # this process's cached device memory back to the server process
     for precision in ("split", "fp64"):
-        reqs = [Request(rid=i, ion=ion, k_max=spec.k_max, arrival=t)
-                for i, ((t, spec), ion) in enumerate(zip(stream, ions))]
-        server = SlaterServer(precision=precision, max_inflight=args.serve_slots, workers=4)
-        # the server warms up on requests of another seed (their grids and
-        # orbital sets differ from the measured stream's, so nothing of the
-        # measured requests is planned or cached ahead): kernels, pinned
-        # staging buffers and the allocator's pools are ready before traffic
-        server.serve([Request(rid=-1 - i, ion=ion, k_max=spec.k_max) for i, (spec, ion) in enumerate(warm)],
-                     realtime=False)
-        torch_sync()
-        rep = server.serve(reqs, realtime=True)
-        server.close()
-        torch_sync()
-        out[precision] = rep.summary()
-        out[precision]["within_p99_bound"] = out[precision]["p99_ms"] <= P99_BOUND_MS
-        errs = [repr(r.error) for r in reqs if r.error is not None]
+        cmd = [sys.executable, "-m", "atomx_b200.serve", "--requests", str(args.serve), "--precision", precision,
+               "--slots", str(args.serve_slots)]
+        proc = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT, timeout=900)
+        try:
+            rep = json.loads(proc.stdout.strip().splitlines()[-1])
+        except (IndexError, ValueError):
+            out[precision] = {"error": f"server exited {proc.returncode}: {proc.stderr.strip()[-300:]}"}
+            continue
+        rep.pop("offline", None)
+        rep.pop("p99_bound_ms", None)
+        errs = rep.pop("errors", [])
         if errs:
-            out[precision]["errors"] = errs[:3]
+            rep["errors"] = errs
+        rep["within_p99_bound"] = rep["p99_ms"] <= P99_BOUND_MS
+        out[precision] = rep
     return out
 
 
