@@ -283,6 +283,35 @@ def _fp64_engine(dev, stream):
     return step, out, ws
 
 
+def _fp64_rows_rate(dev, ws, stream, flush, reps: int = 5) -> dict:
+    """The plain engine's Y^k row kernel alone (g and Y^k rows of the whole
+    table): CUDA events on the launch stream after an L2 flush, median of
+    ``reps``, against the HBM peak.  Algorithmic bytes: the orbital values
+    read once and the g and Y rows written."""
+    import torch
+
+    from atomx_b200 import _native
+    L = _native.load()
+    plan = dev.plan
+    h = _native.stream_handle(stream)
+
+    def launch():
+        _native.check(L.rkb_table_rows_fp64(dev.Pv.data_ptr(), dev.Qv.data_ptr(), dev.n, dev.pairs.data_ptr(),
+                                            dev.row_pair.data_ptr(), dev.row_k.data_ptr(), plan.n_rows,
+                                            dev.r.data_ptr(), dev.w.data_ptr(), dev.nv, dev.ng, dev.mo.data_ptr(),
+                                            dev.mi.data_ptr(), ws.g.data_ptr(), ws.y.data_ptr(), ws.ld, h),
+                      "rkb_table_rows_fp64")
+
+    launch()
+    ms = float(statistics.median(_time_steps(launch, reps, flush, stream)))
+    nbytes = (dev.Pv.numel() + dev.Qv.numel()) * 8 + 2 * plan.n_rows * dev.n * 8
+    peaks, src = measured_peaks()
+    ach = nbytes / (ms / 1e3) / 1e9
+    return {"kernel": "rkb::yk_rows_kernel", "ms": ms, "algorithmic_bytes": int(nbytes), "achieved_gbs": ach,
+            "peak_gbs": float(peaks["hbm_gbs"]), "frac": ach / float(peaks["hbm_gbs"]), "peak_source": src,
+            "timing": f"CUDA events, L2 flushed, median of {reps} launches"}
+
+
 def _time_steps(step, n, flush, stream):
     """Device time (ms) of n steps, each after an L2 flush, CUDA events on stream."""
     import torch
@@ -454,7 +483,8 @@ def run_gpu(args):
             err = table_errors(split_out, out64, eng.offsets, plan)
             gate = 1e-10
             extra["fp64_engine"] = {"ms_per_step": ms64, "value": float(plan.ordered_entries) * world / (ms64 / 1e3),
-                                    "speedup_split_vs_fp64": ms64 / (dev_ms_max / args.steps)}
+                                    "speedup_split_vs_fp64": ms64 / (dev_ms_max / args.steps),
+                                    "row_kernel": _fp64_rows_rate(dev, ws, stream, flush)}
             extra["error_vs_fp64"] = dict(err, gate_schwarz_rel=gate, within_gate=err["max_schwarz_rel"] <= gate)
             del out64, ws
         extra["split"] = eng.info()
