@@ -220,10 +220,23 @@ def _triangle(nt: int) -> np.ndarray:
     return t
 
 
-def tile_tasks(sizes, tile: int = TILE, order=None):
+def tile_tasks(sizes, tile: int = TILE, order=None, block: int | None = None):
     """Upper-triangle tile list [(group, ti, tj)] for groups of the given sizes:
     each group's tiles row-major, groups in order (or in the group order
-    ``order``, a permutation of the group indices)."""
+    ``order``, a permutation of the group indices).
+
+    ``block``: each group's tiles in blocks of block x block tiles instead
+    (blocks row-major, tiles row-major inside a block).  Persistent CTAs take
+    consecutive tasks, so the tiles in flight at one time then read a few
+    row and column panels that stay in L2, where row-major order sweeps a
+    whole tile row of column panels (more than L2 holds on large tables)."""
+    if block is not None:
+        base = tile_tasks(sizes, tile, order)
+        if base.shape[0] == 0:
+            return base
+        g, ti, tj = base[:, 0], base[:, 1], base[:, 2]
+        grank = np.concatenate([[0], np.cumsum(g[1:] != g[:-1])])  # groups are contiguous
+        return base[np.lexsort((tj, ti, tj // block, ti // block, grank))]
     nt = (np.asarray(sizes, dtype=np.int64).reshape(-1) + tile - 1) // tile
     groups = np.arange(nt.shape[0]) if order is None else np.asarray(order, dtype=np.int64)
     groups = groups[nt[groups] > 0]

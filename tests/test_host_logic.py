@@ -34,6 +34,27 @@ def test_tile_tasks_are_each_groups_upper_triangle_in_order():
         assert [tuple(map(int, t)) for t in got] == ref
 
 
+def test_blocked_tile_order_is_a_permutation_by_blocks():
+    """tile_tasks(block=b): every group's upper-triangle tiles, groups still
+    contiguous and in order, tiles ordered by (block row, block column), then
+    row-major inside a block."""
+    from atomx_b200.tables import tile_tasks
+    rng = np.random.default_rng(5)
+    for trial in range(30):
+        sizes = rng.integers(0, 4000, rng.integers(1, 12))
+        for b in (1, 3, 8):
+            base, got = tile_tasks(sizes), tile_tasks(sizes, block=b)
+            assert got.shape == base.shape and got.dtype == np.int32
+            assert sorted(map(tuple, got)) == sorted(map(tuple, base))
+            g = got[:, 0]
+            assert np.all(np.diff(g) >= 0)  # groups contiguous, in order
+            key = np.stack([g, got[:, 1] // b, got[:, 2] // b, got[:, 1], got[:, 2]], axis=1)
+            assert all(tuple(key[i]) < tuple(key[i + 1]) for i in range(len(key) - 1))
+    order = [2, 0, 1]
+    got = tile_tasks([300, 500, 900], order=order, block=2)
+    assert [int(x) for x in dict.fromkeys(got[:, 0])] == order
+
+
 def test_split_width_choice():
     from atomx_b200.split import KDIM_MAX, check_kdim, choose_width
     from atomx_b200.split_plan import MODULI, bits_for_moduli, moduli_needed
