@@ -26,8 +26,7 @@ import numpy as np
 import torch
 
 from . import _native
-from .split_plan import (bits_for_moduli, concat_tables, crt_constants, green_factor_packed, moduli_needed,
-                         table_z_count)
+from .split_plan import bits_for_moduli, crt_constants, green_factor_packed, moduli_needed
 from .tables import Fp64Recompute, IonDevice, tile_tasks
 from .yk import yk_partial_matrices
 
